@@ -1,0 +1,87 @@
+// Problem and tile descriptors shared by the host planner and the sm_100a
+// kernels.  Plain-old-data: passed to kernels by value (single transpose) or
+// stored in a device table (batched / served forms).
+#pragma once
+
+#include <stdint.h>
+
+#define HPTT_MAX_RANK 8
+
+// Element kinds (same numbering as include/hptt_cuda.h).
+enum HpttDtype : int32_t { DT_F32 = 0, DT_F64 = 1, DT_C64 = 2, DT_C128 = 3 };
+
+// Arithmetic modes.
+//   MODE_COPY   alpha == 1 exactly and B not updated: out = a (bit copy; equal
+//               to fl(1*a) for every non-NaN a, and keeps NaN payloads as the
+//               reference's x86 multiply does for quiet NaNs).
+//   MODE_REAL   real scalars; complex types are scaled per component
+//               (reference semantics, inc/hptt/types.h:29-54).
+//   MODE_CPLX   complex scalars for complex types (extension).
+enum HpttMode : int32_t { MODE_COPY = 0, MODE_REAL = 1, MODE_CPLX = 2 };
+
+// Kernel kinds.
+//   KIND_TILE  tiles pair input-contiguous dims (X) with output-contiguous
+//              dims (Y) and go through shared memory.
+//   KIND_ROWS  the fused stride-1 dimension is shared by A and B: rows are
+//              copied/scaled directly, no shared-memory transpose.
+enum HpttKind : int32_t { KIND_TILE = 0, KIND_ROWS = 1 };
+
+// Fused problem.  Dimensions are listed in INPUT order; sA/sB are the strides
+// (in elements) of input dim d in A and in B.  perm[k] = input dim that is
+// output dim k.
+struct HpttProblem {
+  int32_t dtype;
+  int32_t rank;
+  int64_t n[HPTT_MAX_RANK];
+  int64_t sA[HPTT_MAX_RANK];
+  int64_t sB[HPTT_MAX_RANK];
+  int32_t perm[HPTT_MAX_RANK];
+};
+
+// Tile shape and grid decomposition.
+//
+// A tile is W x X x Y elements:
+//   W  the shared stride-1 block (input dim 0 when it is also output dim 0,
+//      else W = 1),
+//   X  input-side dims (input order) after W; all full except the last
+//      (xc, tile extent xt[nx-1]),
+//   Y  output-side dims (output order) after W; all full except the last
+//      (yc).
+// Load phase: element (w, x, y) -> e = w + W*x (RW = W*TX), row y.
+// Store phase: e2 = w + W*y (WTY = W*TY), column x.
+// Shared memory keeps element (w, x, y) at y*LD + e.
+// KIND_ROWS uses W = the row chunk (vector lanes), X empty, Y = other dims.
+struct HpttTile {
+  int32_t kind;
+  int32_t nt;        // threads per CTA
+  int32_t vec;       // elements per vector access (KIND_ROWS only)
+  int32_t W;
+  int32_t nx, ny;
+  int32_t xd[HPTT_MAX_RANK], xt[HPTT_MAX_RANK];
+  int32_t yd[HPTT_MAX_RANK], yt[HPTT_MAX_RANK];
+  int32_t TX, TY, RW, WTY, LD;
+  int32_t R1, J1, R2, J2;     // threads-per-pass mapping, iterations
+  int32_t xc, yc;             // chunked input dims, -1 when none
+  int32_t wc;                 // chunked W dim (KIND_ROWS), -1 when none
+  // grid: tile index -> origin.  gd = input dim, gcnt = number of positions,
+  // gstep = tile extent along that dim (1 for dims outside the tile).
+  int32_t ng;
+  int32_t gd[HPTT_MAX_RANK];
+  uint32_t gcnt[HPTT_MAX_RANK];
+  int32_t gstep[HPTT_MAX_RANK];
+  uint32_t num_tiles;
+  int32_t big_offsets;        // 1 when in-tile offsets need 64 bits
+  int32_t smem_bytes;         // dynamic shared memory for one CTA
+};
+
+// Everything one launch (or one batch entry) needs.
+struct HpttArgs {
+  HpttProblem p;
+  HpttTile t;
+  const void *A;
+  void *B;
+  double alpha[2];
+  double beta[2];
+  int32_t mode;
+  int32_t update;
+};
