@@ -1,0 +1,469 @@
+#!/usr/bin/env python3
+"""Benchmark: B = alpha * A(perm) + beta * B on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload sweep|plain|hard]
+
+Default workload ("sweep"): the plain permutation sweep -- 48 seeded cases over
+ranks 2-6 in f32/f64, random non-identity permutations, extents log-uniform in
+[4, 4096] rescaled to ~200 MB per tensor, each run with alpha=1, beta=0 and
+with alpha=2.3, beta=4.2.  One step = all 96 transposes, every tensor resident
+in HBM (19.2 GB); tensors are larger than L2, so no L2 flush is needed.
+
+value     = algorithmic bytes of all transposes of all ranks / max-over-ranks
+            device time (bytes = 2*N*sizeof(T), + N*sizeof(T) when B is read)
+e2e       = the same metric through the C ABI with host buffers: every step
+            copies A (and B when it is read) from pinned host memory, runs
+            exec, and copies B back, all inside the timed region
+roofline  = the dominant kernel's achieved bandwidth over the measured HBM
+            copy peak (MEASURED_PEAKS.json)
+cpu_baseline = the reference's own CPU plan (oracle/_ref, built from the
+            reference sources) on a bounded sample of the same workload, all
+            host threads; shapes where the reference plan is incorrect are
+            timed with the reference's naive RefTrans instead, labelled.
+
+N > 1 (torchrun): every rank runs the whole workload on its own GPU
+(independent transposes; no collective on the data path), scaling "weak".
+`--impl reference` times only the reference's CPU implementation (rank 0).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "GB/s & % HBM peak per transpose; batched req/s + p99 vs plain per-call exec"
+
+
+def _peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def _workload(name):
+    from hptt_b200 import workloads as w
+    if name == "sweep":
+        cases = []
+        for c in w.sweep_cases():
+            cases.append(dict(c, alpha=1.0, beta=0.0))
+            cases.append(dict(c, alpha=2.3, beta=4.2))
+        return cases, "permutation sweep: 48 cases (ranks 2-6, f32/f64, ~200 MB/tensor) x {a=1,b=0; a=2.3,b=4.2}"
+    if name == "plain":
+        return [w.plain_single()], "f32 {256,256,256} perm {2,1,0} a=2.3 b=4.2"
+    if name == "hard":
+        return w.hard_cases(), "c64/c128 rank-6 hard layouts, complex scalars"
+    raise SystemExit(f"unknown workload {name}")
+
+
+# --------------------------------------------------------------------------
+# clocks
+# --------------------------------------------------------------------------
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.dev = device_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.dev), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# --------------------------------------------------------------------------
+# our arm
+# --------------------------------------------------------------------------
+def _tdtype(torch, name):
+    return {"f32": torch.float32, "f64": torch.float64, "c64": torch.complex64,
+            "c128": torch.complex128}[name]
+
+
+def run_ours(args, rank, world, dist):
+    import torch
+    import hptt_b200 as h
+    from hptt_b200.workloads import algorithmic_bytes
+
+    dev = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(dev)
+    cases, desc = _workload(args.workload)
+    stream = torch.cuda.current_stream()
+
+    # resident buffers: one A and one B per distinct tensor shape
+    bufs = {}
+    plans = []
+    g = torch.Generator(device="cuda").manual_seed(1234 + rank)
+    for c in cases:
+        key = (c["dtype"], tuple(c["in_size"]), tuple(c["perm"]))
+        if key not in bufs:
+            n = int(np.prod(c["in_size"]))
+            t = _tdtype(torch, c["dtype"])
+            if c["dtype"] in ("c64", "c128"):
+                rt = torch.float32 if c["dtype"] == "c64" else torch.float64
+                a = torch.view_as_complex((torch.rand(n, 2, generator=g, device="cuda", dtype=rt) * 2 - 1).contiguous())
+                b = torch.view_as_complex((torch.rand(n, 2, generator=g, device="cuda", dtype=rt) * 2 - 1).contiguous())
+            else:
+                a = torch.rand(n, generator=g, device="cuda", dtype=t) * 2 - 1
+                b = torch.rand(n, generator=g, device="cuda", dtype=t) * 2 - 1
+            bufs[key] = (a, b)
+        a, b = bufs[key]
+        p = h.create_plan(a, b, c["in_size"], c["perm"], c["alpha"], c["beta"], 0,
+                          dtype=c["dtype"])
+        assert p is not None
+        kind = "rows" if "kernel: rows" in p.describe() else "tile"
+        plans.append((p, algorithmic_bytes(c), kind, c))
+    torch.cuda.synchronize()
+    sptr = stream.cuda_stream
+
+    def step(record=None):
+        for i, (p, _, _, _) in enumerate(plans):
+            if record is not None:
+                record[i][0].record(stream)
+            p.exec_on(sptr)
+            if record is not None:
+                record[i][1].record(stream)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    sampler = ClockSampler(dev)
+    sampler.start()
+    ev = [[(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+           for _ in plans] for _ in range(args.steps)]
+    t0 = torch.cuda.Event(enable_timing=True)
+    t1 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    t0.record(stream)
+    for k in range(args.steps):
+        step(ev[k])
+    t1.record(stream)
+    torch.cuda.synchronize()
+    clocks = sampler.stop()
+    elapsed_ms = t0.elapsed_time(t1)
+    per_launch_ms = [sum(ev[k][i][0].elapsed_time(ev[k][i][1]) for k in range(args.steps))
+                     for i in range(len(plans))]
+    if world > 1:
+        tt = torch.tensor([elapsed_ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        elapsed_ms = float(tt[0])
+    device_ms = sum(per_launch_ms)
+
+    bytes_step = sum(bb for _, bb, _, _ in plans)
+    total_bytes = bytes_step * args.steps * world
+    value = total_bytes / (elapsed_ms / 1e3) / 1e9
+    ms_per_step = elapsed_ms / args.steps
+
+    # dominant kernel: the kernel kind with the most device time
+    by_kind = {}
+    for (p, bb, kind, _), ms in zip(plans, per_launch_ms):
+        d = by_kind.setdefault(kind, [0.0, 0, 0])
+        d[0] += ms
+        d[1] += bb * args.steps
+        d[2] += args.steps
+    dom = max(by_kind, key=lambda k: by_kind[k][0])
+    dom_ms, dom_bytes, dom_launches = by_kind[dom]
+    peak, peak_kind = _peaks()
+    achieved = dom_bytes / (dom_ms / 1e3) / 1e9
+    traffic = _profiled_traffic(dom)
+    roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak,
+                "unit": "GB/s", "frac": round(achieved / peak, 4),
+                "traffic": traffic, "kernel": "k_tile" if dom == "tile" else "k_rows",
+                "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs, burst copy)",
+                "launches": dom_launches,
+                "share_of_device_time": round(dom_ms / device_ms, 4)}
+
+    e2e = run_e2e(args, plans, bufs, stream) if args.e2e_steps > 0 else None
+    gpu_launches = sum(p.launches for p, _, _, _ in plans) * args.steps
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline_sample(cases, budget_s=args.cpu_budget)
+
+    out = {
+        "metric": METRIC, "value": round(value, 1), "unit": "GB/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_per_step, 4),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32+f64" if args.workload == "sweep" else cases[0]["dtype"],
+        "data": "synthetic (seeded uniform[-1,1]; shapes from the workload generator)",
+        "config": {"workload": desc, "transposes_per_step": len(plans),
+                   "bytes_per_step": bytes_step, "l2": "inputs larger than L2 (no flush)",
+                   "parallelism": f"replicas x{world}"},
+        "hbm_frac": round(value / world / peak, 4),
+        "roofline": roofline,
+        "e2e": e2e,
+        "gpu_launches": gpu_launches,
+        "clocks": clocks,
+        "cpu_baseline": cpu,
+        "kernel_ms_per_step": round(device_ms / args.steps, 4),
+    }
+    return out
+
+
+def _profiled_traffic(kind):
+    """DRAM bytes per launch of the dominant kernel from the committed ncu
+    summary (profiles/*.json), when one exists."""
+    p = os.path.join(ROOT, "profiles", "traffic.json")
+    if not os.path.exists(p):
+        return None
+    try:
+        d = json.load(open(p))
+        return d.get(kind)
+    except Exception:
+        return None
+
+
+def run_e2e(args, plans, bufs, stream):
+    """Same workload through the C ABI with host buffers, copies timed."""
+    import torch
+    # pinned host staging, one set per distinct tensor size (reused)
+    host = {}
+    for key, (a, b) in bufs.items():
+        host[key] = (torch.empty_like(a, device="cpu").pin_memory(),
+                     torch.empty_like(b, device="cpu").pin_memory(),
+                     torch.empty_like(b, device="cpu").pin_memory())
+        host[key][0].copy_(a.cpu())
+        host[key][1].copy_(b.cpu())
+    h2d = d2h = 0
+    keys = []
+    for p, bb, kind, c in plans:
+        key = (c["dtype"], tuple(c["in_size"]), tuple(c["perm"]))
+        keys.append(key)
+        nbytes = bufs[key][0].numel() * bufs[key][0].element_size()
+        reads_b = bb > 2 * nbytes
+        h2d += nbytes * (2 if reads_b else 1)
+        d2h += nbytes
+
+    def step():
+        for (p, bb, kind, c), key in zip(plans, keys):
+            a, b = bufs[key]
+            ha, hb, hout = host[key]
+            a.copy_(ha, non_blocking=True)
+            if bb > 2 * a.numel() * a.element_size():
+                b.copy_(hb, non_blocking=True)
+            p.exec_on(stream.cuda_stream)
+            hout.copy_(b, non_blocking=True)
+
+    for _ in range(min(1, args.warmup)):
+        step()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.e2e_steps):
+        step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    total = sum(bb for _, bb, _, _ in plans) * args.e2e_steps
+    return {"value": round(total / (ms / 1e3) / 1e9, 2), "unit": "GB/s",
+            "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+            "steps": args.e2e_steps, "ms_per_step": round(ms / args.e2e_steps, 3),
+            "api": "hptt_cuda_plan_exec_on (C ABI) + pinned host<->device copies"}
+
+
+# --------------------------------------------------------------------------
+# CPU reference
+# --------------------------------------------------------------------------
+def _host_has_avx2():
+    try:
+        return "avx2" in open("/proc/cpuinfo").read()
+    except Exception:
+        return False
+
+
+def _fill(x: np.ndarray, seed: int):
+    """Cheap deterministic fill: a small random block tiled over the buffer."""
+    rng = np.random.default_rng(seed)
+    blk = rng.uniform(-1, 1, 1 << 16)
+    flat = x.view(np.float32 if x.dtype in (np.float32, np.complex64) else np.float64)
+    reps = -(-flat.size // blk.size)
+    flat[:] = np.tile(blk.astype(flat.dtype), reps)[:flat.size]
+
+
+def reference_time_case(c, threads, repeat=2):
+    """Best-of-`repeat` time of one case on the reference's CPU code."""
+    import oracle
+    name = c["dtype"]
+    n = int(np.prod(c["in_size"]))
+    a = oracle.aligned_empty(n, oracle.NP_DTYPES[name])
+    b = oracle.aligned_empty(n, oracle.NP_DTYPES[name])
+    _fill(a, 1)
+    _fill(b, 2)
+    al, be = c["alpha"], c["beta"]
+    if isinstance(al, complex) or isinstance(be, complex):
+        # complex scalars are not expressible through the reference API: time
+        # the reference naive transpose with the real parts (same traffic)
+        t = oracle.ref_naive_exec(a, b, c["in_size"], c["perm"], complex(al).real,
+                                  complex(be).real, threads=threads, repeat=repeat)
+        return t, "naive"
+    if oracle.ref_plan_is_safe(name, c["in_size"], c["perm"], be):
+        t = oracle.ref_plan_exec(a, b, c["in_size"], c["perm"], al, be, threads=threads,
+                                 repeat=repeat)
+        return t, "plan"
+    t = oracle.ref_naive_exec(a, b, c["in_size"], c["perm"], al, be, threads=threads,
+                              repeat=repeat)
+    return t, "naive"
+
+
+def cpu_baseline_sample(cases, budget_s=20.0, threads=None):
+    import oracle
+    from hptt_b200.workloads import algorithmic_bytes
+    if not oracle.ref_available() or not _host_has_avx2():
+        return {"value": None, "unit": "GB/s", "cores": 0, "kind": "reference",
+                "sample": "unavailable: reference library not built or host lacks AVX2"}
+    threads = threads or os.cpu_count() or 1
+    t_start = time.time()
+    tot_b = tot_t = 0.0
+    used = {"plan": 0, "naive": 0}
+    done = 0
+    order = list(range(0, len(cases), 7)) + [i for i in range(len(cases)) if i % 7]
+    for i in order:
+        if time.time() - t_start > budget_s:
+            break
+        t, how = reference_time_case(cases[i], threads)
+        tot_b += algorithmic_bytes(cases[i])
+        tot_t += t
+        used[how] += 1
+        done += 1
+    return {"value": round(tot_b / tot_t / 1e9, 2) if tot_t else None, "unit": "GB/s",
+            "cores": threads, "kind": "reference",
+            "sample": (f"{done} of {len(cases)} transposes of the same workload, best of 2 execs "
+                       f"each, {threads} OpenMP threads; {used['plan']} by the reference plan, "
+                       f"{used['naive']} by the reference's naive RefTrans (plan incorrect on "
+                       f"those shapes or complex scalars)")}
+
+
+def run_reference(args):
+    import oracle
+    from hptt_b200.workloads import algorithmic_bytes
+    cases, desc = _workload(args.workload)
+    threads = os.cpu_count() or 1
+    if not oracle.ref_available():
+        return {"impl": "reference", "unavailable": "oracle/_ref/libhptt_ref.so not built"}
+    if not _host_has_avx2():
+        return {"impl": "reference", "unavailable": "host CPU lacks AVX2 (reference AVX2 build)"}
+    # each step: a rotating sample of cases (bounded CPU time)
+    per_step = max(1, min(len(cases), args.ref_cases_per_step))
+    tot_b = tot_t = 0.0
+    used = {"plan": 0, "naive": 0}
+    idx = 0
+    for s in range(args.warmup + args.steps):
+        for _ in range(per_step):
+            c = cases[idx % len(cases)]
+            idx += 1
+            t, how = reference_time_case(c, threads, repeat=1)
+            if s >= args.warmup:
+                tot_b += algorithmic_bytes(c)
+                tot_t += t
+                used[how] += 1
+    value = tot_b / tot_t / 1e9 if tot_t else None
+    sample = (f"{per_step} transposes per step (rotating through the workload), "
+              f"{used['plan']} by the reference plan, {used['naive']} by the reference's "
+              f"naive RefTrans (plan incorrect on those shapes)")
+    return {
+        "impl": "reference", "metric": METRIC, "value": round(value, 2) if value else None,
+        "unit": "GB/s", "n_gpus": 0, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(tot_t * 1e3 / max(1, args.steps), 3),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32+f64" if args.workload == "sweep" else cases[0]["dtype"],
+        "data": "synthetic", "config": {"workload": desc, "threads": threads},
+        "cpu_baseline": {"value": round(value, 2) if value else None, "unit": "GB/s",
+                         "cores": threads, "kind": "reference", "sample": sample},
+        "e2e": {"value": round(value, 2) if value else None, "unit": "GB/s",
+                "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="sweep", choices=["sweep", "plain", "hard"])
+    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--cpu-budget", type=float, default=20.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--ref-cases-per-step", type=int, default=4)
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if args.impl == "reference":
+        if rank == 0:
+            print(json.dumps(run_reference(args)), flush=True)
+        return
+    dist = None
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    try:
+        out = run_ours(args, rank, world, dist)
+    finally:
+        if dist is not None:
+            dist.barrier()
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,292 @@
+"""hptt_b200 -- B200 (sm_100a) tensor transposition B = alpha * A(perm) + beta * B.
+
+Python mirror of the reference's plan interface, bound to the C ABI of
+``libhptt_cuda.so`` (include/hptt_cuda.h) with ctypes:
+
+    plan = hptt_b200.create_plan(a, b, in_size, perm, alpha, beta, num_threads)
+    if plan is not None:
+        plan.exec()
+
+``create_plan`` mirrors ``hptt::create_plan`` (reference inc/hptt/hptt.h:85-93):
+same argument meaning and order, and ``None`` where the reference returns
+``nullptr`` (invalid arguments, inc/hptt/hptt.h:71-83).  The plan object has the
+reference's methods ``exec``, ``__call__``, ``print_plan``, ``reset_data``,
+``set_thread_ids`` and ``unset_thread_ids`` (inc/hptt/impl/hptt_trans.h:26-31),
+plus ``sync`` and ``set_stream`` because ``exec`` is asynchronous on the GPU.
+
+Data are device buffers: torch CUDA tensors, objects exposing
+``__cuda_array_interface__``, or raw device addresses (int).  Tensors are flat
+column-major buffers: dimension 0 has stride 1.
+
+There is no CPU fallback: importing works anywhere, but creating a plan needs
+the compiled library and a CUDA device, and raises if either is missing.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from typing import Optional, Sequence
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libhptt_cuda.so")
+
+F32, F64, C64, C128 = 0, 1, 2, 3
+_DTYPE_NAMES = {"f32": F32, "float32": F32, "float": F32,
+                "f64": F64, "float64": F64, "double": F64,
+                "c64": C64, "complex64": C64, "cfloat": C64,
+                "c128": C128, "complex128": C128, "cdouble": C128}
+ELEM_BYTES = {F32: 4, F64: 8, C64: 8, C128: 16}
+
+STATUS = {
+    0: "ok", 1: "null data pointer", 2: "bad rank", 3: "bad size vector",
+    4: "bad size value", 5: "bad permutation", 6: "bad dtype", 7: "CUDA error",
+    8: "no CUDA device", 9: "allocation failed", 10: "memory budget exceeded",
+    11: "invalid handle", 12: "timeout", 13: "too large", 14: "busy",
+}
+# argument errors for which the reference returns nullptr
+_NULLPTR_STATUSES = {1, 2, 3, 4, 5}
+
+
+class HpttError(RuntimeError):
+    def __init__(self, status: int, what: str = ""):
+        self.status = status
+        super().__init__(f"{what}: {STATUS.get(status, status)} ({status})")
+
+
+_lib = None
+_u32p = ctypes.POINTER(ctypes.c_uint32)
+_dp = ctypes.POINTER(ctypes.c_double)
+
+
+def library_path() -> str:
+    return LIB_PATH
+
+
+def load_library() -> ctypes.CDLL:
+    """Load libhptt_cuda.so (raises if it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError(
+            f"{LIB_PATH} is missing: build it with `python -m hptt_b200.build`")
+    lib = ctypes.CDLL(LIB_PATH)
+    c_int, c_u32, c_vp, c_dbl, c_sz = (ctypes.c_int, ctypes.c_uint32, ctypes.c_void_p,
+                                       ctypes.c_double, ctypes.c_size_t)
+    sigs = {
+        "hptt_cuda_plan_create": (c_int, [c_int, c_u32, _u32p, _u32p, _u32p, _u32p, _dp, _dp,
+                                          c_int, c_vp, c_vp, c_u32, c_dbl,
+                                          ctypes.POINTER(c_vp)]),
+        "hptt_cuda_plan_exec": (c_int, [c_vp]),
+        "hptt_cuda_plan_exec_on": (c_int, [c_vp, c_vp]),
+        "hptt_cuda_plan_reset_data": (c_int, [c_vp, c_vp, c_vp]),
+        "hptt_cuda_plan_describe": (c_int, [c_vp, ctypes.c_char_p, c_sz]),
+        "hptt_cuda_plan_set_thread_ids": (c_int, [c_vp, ctypes.POINTER(ctypes.c_int32), c_u32]),
+        "hptt_cuda_plan_unset_thread_ids": (c_int, [c_vp]),
+        "hptt_cuda_plan_set_stream": (c_int, [c_vp, c_vp]),
+        "hptt_cuda_plan_sync": (c_int, [c_vp]),
+        "hptt_cuda_plan_set_coef": (c_int, [c_vp, _dp, _dp, c_int]),
+        "hptt_cuda_plan_bytes": (c_int, [c_vp, ctypes.POINTER(ctypes.c_uint64)]),
+        "hptt_cuda_plan_launches": (c_int, [c_vp, ctypes.POINTER(c_u32)]),
+        "hptt_cuda_plan_destroy": (c_int, [c_vp]),
+        "hptt_cuda_plan_inspect": (c_int, [c_int, c_u32, _u32p, _u32p, _u32p, _u32p,
+                                           ctypes.c_char_p, c_sz]),
+        "hptt_cuda_status_string": (ctypes.c_char_p, [c_int]),
+        "hptt_cuda_version": (ctypes.c_char_p, []),
+    }
+    for name, (res, args) in sigs.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+def _u32(v: Optional[Sequence[int]]):
+    if v is None:
+        return None
+    return (ctypes.c_uint32 * len(v))(*[int(x) for x in v])
+
+
+def _scalar(x) -> ctypes.Array:
+    z = complex(x)
+    return (ctypes.c_double * 2)(z.real, z.imag)
+
+
+def _device_ptr(x) -> int:
+    if x is None:
+        return 0
+    if isinstance(x, int):
+        return x
+    iface = getattr(x, "__cuda_array_interface__", None)
+    if iface is not None:
+        return int(iface["data"][0])
+    if hasattr(x, "data_ptr"):
+        return int(x.data_ptr())
+    raise TypeError(f"cannot take a device address of {type(x)!r}")
+
+
+def dtype_code(x) -> int:
+    """Element type code from a name, a torch dtype/tensor or a numpy dtype."""
+    if isinstance(x, int):
+        return x
+    if isinstance(x, str):
+        return _DTYPE_NAMES[x]
+    dt = getattr(x, "dtype", x)
+    name = str(dt).replace("torch.", "")
+    if name in _DTYPE_NAMES:
+        return _DTYPE_NAMES[name]
+    raise TypeError(f"unsupported element type {dt!r}")
+
+
+class TransPlan:
+    """A transpose plan bound to device buffers (reference ``trans_plan<T>``)."""
+
+    def __init__(self, handle: int, dtype: int, keep=()):
+        self._h = ctypes.c_void_p(handle)
+        self.dtype = dtype
+        self._keep = list(keep)  # keep tensors alive while the plan holds them
+
+    # -- reference interface (inc/hptt/impl/hptt_trans.h:26-31) --
+    def exec(self) -> None:
+        self._check(load_library().hptt_cuda_plan_exec(self._h), "exec")
+
+    def __call__(self) -> None:
+        self.exec()
+
+    def print_plan(self) -> None:
+        print(self.describe(), end="")
+
+    def reset_data(self, in_data, out_data) -> None:
+        self._check(load_library().hptt_cuda_plan_reset_data(
+            self._h, _device_ptr(in_data), _device_ptr(out_data)), "reset_data")
+        self._keep = [in_data, out_data]
+
+    def set_thread_ids(self, thread_ids: Sequence[int]) -> None:
+        arr = (ctypes.c_int32 * len(thread_ids))(*thread_ids)
+        self._check(load_library().hptt_cuda_plan_set_thread_ids(self._h, arr, len(thread_ids)),
+                    "set_thread_ids")
+
+    def unset_thread_ids(self) -> None:
+        self._check(load_library().hptt_cuda_plan_unset_thread_ids(self._h), "unset_thread_ids")
+
+    # -- extensions --
+    def exec_on(self, stream) -> None:
+        self._check(load_library().hptt_cuda_plan_exec_on(self._h, _stream_ptr(stream)),
+                    "exec_on")
+
+    def set_stream(self, stream) -> None:
+        self._check(load_library().hptt_cuda_plan_set_stream(self._h, _stream_ptr(stream)),
+                    "set_stream")
+
+    def sync(self) -> None:
+        self._check(load_library().hptt_cuda_plan_sync(self._h), "sync")
+
+    def set_coef(self, alpha, beta, complex_scalars: bool = False) -> None:
+        self._check(load_library().hptt_cuda_plan_set_coef(
+            self._h, _scalar(alpha), _scalar(beta), int(complex_scalars)), "set_coef")
+
+    def describe(self) -> str:
+        buf = ctypes.create_string_buffer(4096)
+        self._check(load_library().hptt_cuda_plan_describe(self._h, buf, 4096), "describe")
+        return buf.value.decode()
+
+    @property
+    def bytes(self) -> int:
+        v = ctypes.c_uint64(0)
+        self._check(load_library().hptt_cuda_plan_bytes(self._h, ctypes.byref(v)), "bytes")
+        return int(v.value)
+
+    @property
+    def launches(self) -> int:
+        v = ctypes.c_uint32(0)
+        self._check(load_library().hptt_cuda_plan_launches(self._h, ctypes.byref(v)), "launches")
+        return int(v.value)
+
+    @property
+    def handle(self) -> int:
+        return int(self._h.value or 0)
+
+    def destroy(self) -> None:
+        if self._h and self._h.value:
+            load_library().hptt_cuda_plan_destroy(self._h)
+            self._h = ctypes.c_void_p(0)
+
+    def __del__(self):
+        try:
+            self.destroy()
+        except Exception:
+            pass
+
+    @staticmethod
+    def _check(st: int, what: str) -> None:
+        if st != 0:
+            raise HpttError(st, what)
+
+
+def _stream_ptr(stream) -> int:
+    if stream is None:
+        return 0
+    if isinstance(stream, int):
+        return stream
+    return int(getattr(stream, "cuda_stream"))
+
+
+def create_plan(in_data, out_data, in_size: Sequence[int], perm: Sequence[int],
+                alpha, beta, num_threads: int = 0, tuning_timeout: float = 0.0,
+                in_outer_size: Sequence[int] = (), out_outer_size: Sequence[int] = (),
+                dtype=None, complex_scalars: Optional[bool] = None) -> Optional[TransPlan]:
+    """Mirror of ``hptt::create_plan`` (reference inc/hptt/hptt.h:85-93).
+
+    Returns ``None`` exactly where the reference returns ``nullptr``: a null
+    data pointer, rank < 2, a size vector of the wrong length, a zero extent or
+    an outer size below the inner size, or an invalid permutation.  Device or
+    library failures raise :class:`HpttError`.
+
+    ``alpha``/``beta`` are real scalars as in the reference; for complex
+    element types a Python complex (or ``complex_scalars=True``) selects the
+    complex-scalar extension.
+    """
+    code = dtype_code(dtype if dtype is not None else in_data)
+    rank = len(perm)
+    if rank <= 1:
+        return None
+    if len(in_size) != rank:
+        return None
+    if (len(in_outer_size) not in (0, rank)) or (len(out_outer_size) not in (0, rank)):
+        return None
+    ip, op = _device_ptr(in_data), _device_ptr(out_data)
+    if complex_scalars is None:
+        complex_scalars = code in (C64, C128) and (
+            isinstance(alpha, complex) or isinstance(beta, complex))
+    lib = load_library()
+    h = ctypes.c_void_p(0)
+    st = lib.hptt_cuda_plan_create(
+        code, rank, _u32(in_size), _u32(perm),
+        _u32(in_outer_size) if len(in_outer_size) else None,
+        _u32(out_outer_size) if len(out_outer_size) else None,
+        _scalar(alpha), _scalar(beta), int(bool(complex_scalars)),
+        ip, op, int(num_threads), float(tuning_timeout), ctypes.byref(h))
+    if st in _NULLPTR_STATUSES:
+        return None
+    if st != 0:
+        raise HpttError(st, "create_plan")
+    return TransPlan(h.value, code, keep=(in_data, out_data))
+
+
+def inspect_plan(dtype, in_size: Sequence[int], perm: Sequence[int],
+                 in_outer_size: Sequence[int] = (), out_outer_size: Sequence[int] = ()) -> str:
+    """Host-only dry run of the planner (no device, no data)."""
+    lib = load_library()
+    buf = ctypes.create_string_buffer(4096)
+    st = lib.hptt_cuda_plan_inspect(
+        dtype_code(dtype), len(perm), _u32(in_size), _u32(perm),
+        _u32(in_outer_size) if len(in_outer_size) else None,
+        _u32(out_outer_size) if len(out_outer_size) else None, buf, 4096)
+    if st != 0:
+        raise HpttError(st, "inspect_plan")
+    return buf.value.decode()
+
+
+def version() -> str:
+    return load_library().hptt_cuda_version().decode()

@@ -1,0 +1,213 @@
+// Tile-shape autotuner and its cache.
+#include "autotune.h"
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <fstream>
+#include <map>
+#include <mutex>
+#include <sstream>
+#include <vector>
+
+#include "launch.h"
+
+namespace hptt_b200 {
+
+namespace {
+
+std::mutex g_mu;
+std::map<std::string, TileParams> g_cache;
+bool g_loaded = false;
+
+std::string gpu_name() {
+  int dev = 0;
+  cudaDeviceProp prop;
+  if (cudaGetDevice(&dev) != cudaSuccess) return "unknown";
+  if (cudaGetDeviceProperties(&prop, dev) != cudaSuccess) return "unknown";
+  std::string s = prop.name;
+  std::replace(s.begin(), s.end(), ' ', '_');
+  return s;
+}
+
+const char *env_path() { return std::getenv("HPTT_B200_TUNE_CACHE"); }
+
+void ensure_loaded() {
+  if (g_loaded) return;
+  g_loaded = true;
+  const char *p = env_path();
+  if (!p) return;
+  std::ifstream f(p);
+  std::string line;
+  while (std::getline(f, line)) {
+    const auto bar = line.find('|');
+    if (bar == std::string::npos) continue;
+    std::istringstream v(line.substr(bar + 1));
+    TileParams tp;
+    if (v >> tp.run_bytes >> tp.vmin_bytes >> tp.smem_bytes >> tp.rows_min_bytes >>
+        tp.ctas_per_sm)
+      g_cache[line.substr(0, bar)] = tp;
+  }
+}
+
+int write_cache(const char *path) {
+  std::ofstream f(path, std::ios::trunc);
+  if (!f) return ST_ALLOC;
+  for (const auto &kv : g_cache)
+    f << kv.first << "|" << kv.second.run_bytes << " " << kv.second.vmin_bytes << " "
+      << kv.second.smem_bytes << " " << kv.second.rows_min_bytes << " "
+      << kv.second.ctas_per_sm << "\n";
+  return ST_OK;
+}
+
+std::vector<TileParams> candidates() {
+  std::vector<TileParams> c;
+  for (int run : {256, 128, 512})
+    for (int vmin : {16384, 8192, 32768})
+      for (int cps : {0, 4, 2}) {
+        TileParams tp;
+        tp.run_bytes = run;
+        tp.vmin_bytes = vmin;
+        tp.ctas_per_sm = cps;
+        c.push_back(tp);
+      }
+  return c;
+}
+
+}  // namespace
+
+std::string autotune_key(const Plan *p) {
+  const HpttProblem &q = p->args.p;
+  const uint64_t bytes = p->elements * static_cast<uint64_t>(elem_bytes(q.dtype));
+  const int size_class = bytes ? static_cast<int>(std::floor(std::log2(static_cast<double>(bytes)))) : 0;
+  std::ostringstream os;
+  os << gpu_name() << " " << q.dtype << " " << q.rank << " ";
+  for (int k = 0; k < q.rank; ++k) os << q.perm[k] << (k + 1 < q.rank ? "," : "");
+  os << " " << size_class << " " << p->args.update;
+  return os.str();
+}
+
+bool autotune_cache_lookup(const Plan *p, TileParams *out) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  ensure_loaded();
+  auto it = g_cache.find(autotune_key(p));
+  if (it == g_cache.end()) return false;
+  *out = it->second;
+  return true;
+}
+
+int autotune(Plan *p, double timeout, TileParams *best) {
+  // scratch output with B's footprint
+  const HpttProblem &q = p->args.p;
+  int64_t span = 1;
+  for (int d = 0; d < q.rank; ++d) span += (q.n[d] - 1) * q.sB[d];
+  const size_t bytes = static_cast<size_t>(span) * elem_bytes(q.dtype);
+  void *scratch = nullptr;
+  if (cudaMalloc(&scratch, bytes) != cudaSuccess) {
+    cudaGetLastError();
+    return ST_ALLOC;
+  }
+  cudaStream_t s = nullptr;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  int st = ST_OK;
+  if (cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess ||
+      cudaMemsetAsync(scratch, 0, bytes, s) != cudaSuccess) {
+    st = ST_CUDA;
+  }
+  const auto t_start = std::chrono::steady_clock::now();
+  float best_ms = 1e30f;
+  TileParams winner;
+  bool found = false;
+  void *user_B = p->args.B;
+  p->args.B = scratch;
+  for (const TileParams &tp : candidates()) {
+    if (st != ST_OK) break;
+    if (timeout > 0) {
+      const double el = std::chrono::duration<double>(std::chrono::steady_clock::now() - t_start).count();
+      if (el > timeout) break;
+    }
+    if (plan_tiles(p, tp) != ST_OK) continue;
+    if (plan_enqueue(p, s) != ST_OK) continue;  // warm-up
+    float ms_best = 1e30f;
+    for (int r = 0; r < 3; ++r) {
+      cudaEventRecord(e0, s);
+      plan_enqueue(p, s);
+      cudaEventRecord(e1, s);
+      if (cudaEventSynchronize(e1) != cudaSuccess) {
+        st = ST_CUDA;
+        break;
+      }
+      float ms = 0;
+      cudaEventElapsedTime(&ms, e0, e1);
+      ms_best = std::min(ms_best, ms);
+    }
+    if (ms_best < best_ms) {
+      best_ms = ms_best;
+      winner = tp;
+      found = true;
+    }
+  }
+  p->args.B = user_B;
+  if (s) cudaStreamSynchronize(s);
+  if (e0) cudaEventDestroy(e0);
+  if (e1) cudaEventDestroy(e1);
+  if (s) cudaStreamDestroy(s);
+  cudaFree(scratch);
+  if (st != ST_OK) return st;
+  if (!found) return ST_TOO_LARGE;
+  *best = winner;
+  p->tuned = true;
+  std::lock_guard<std::mutex> lk(g_mu);
+  ensure_loaded();
+  g_cache[autotune_key(p)] = winner;
+  if (const char *path = env_path()) write_cache(path);
+  return ST_OK;
+}
+
+int autotune_cache_load(const char *path) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  if (!path) {
+    g_loaded = false;
+    ensure_loaded();
+    return ST_OK;
+  }
+  std::ifstream f(path);
+  if (!f) return ST_ALLOC;
+  std::string line;
+  while (std::getline(f, line)) {
+    const auto bar = line.find('|');
+    if (bar == std::string::npos) continue;
+    std::istringstream v(line.substr(bar + 1));
+    TileParams tp;
+    if (v >> tp.run_bytes >> tp.vmin_bytes >> tp.smem_bytes >> tp.rows_min_bytes >>
+        tp.ctas_per_sm)
+      g_cache[line.substr(0, bar)] = tp;
+  }
+  g_loaded = true;
+  return ST_OK;
+}
+
+int autotune_cache_save(const char *path) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  const char *p = path ? path : env_path();
+  if (!p) return ST_OK;
+  return write_cache(p);
+}
+
+void autotune_cache_clear() {
+  std::lock_guard<std::mutex> lk(g_mu);
+  g_cache.clear();
+  g_loaded = true;
+}
+
+int autotune_cache_size() {
+  std::lock_guard<std::mutex> lk(g_mu);
+  return static_cast<int>(g_cache.size());
+}
+
+}  // namespace hptt_b200

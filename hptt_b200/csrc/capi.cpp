@@ -1,0 +1,279 @@
+// C ABI of libhptt_cuda.so: single-transpose plans.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+
+#include "../../include/hptt_cuda.h"
+#include "autotune.h"
+#include "launch.h"
+#include "plan.h"
+#include "planner.h"
+
+namespace hptt_b200 {
+
+bool plan_valid(const Plan *p) { return p && p->magic == kPlanMagic; }
+
+void set_scalars(HpttArgs *a, const double *alpha, const double *beta,
+                 int complex_scalars) {
+  const bool cplx_type = a->p.dtype == DT_C64 || a->p.dtype == DT_C128;
+  const bool use_cplx = cplx_type && complex_scalars;
+  a->alpha[0] = alpha[0];
+  a->alpha[1] = use_cplx ? alpha[1] : 0.0;
+  a->beta[0] = beta[0];
+  a->beta[1] = use_cplx ? beta[1] : 0.0;
+  // Update rule: |beta| >= 1e-16 (inc/hptt/impl/hptt_trans_impl.h:75-78), on
+  // the scalar in the element's precision.
+  bool upd;
+  if (use_cplx) {
+    upd = std::fabs(a->beta[0]) >= 1e-16 || std::fabs(a->beta[1]) >= 1e-16;
+  } else if (a->p.dtype == DT_F32 || a->p.dtype == DT_C64) {
+    upd = std::fabs(static_cast<float>(a->beta[0])) >= 1e-16;
+  } else {
+    upd = std::fabs(a->beta[0]) >= 1e-16;
+  }
+  a->update = upd ? 1 : 0;
+  const bool alpha_one = use_cplx ? (a->alpha[0] == 1.0 && a->alpha[1] == 0.0)
+                                  : ((a->p.dtype == DT_F32 || a->p.dtype == DT_C64)
+                                         ? static_cast<float>(a->alpha[0]) == 1.0f
+                                         : a->alpha[0] == 1.0);
+  if (!upd && alpha_one)
+    a->mode = MODE_COPY;
+  else
+    a->mode = use_cplx ? MODE_CPLX : MODE_REAL;
+}
+
+int plan_tiles(Plan *p, const TileParams &params) {
+  p->params = params;
+  int st = choose_tile(p->args.p, params, &p->args.t);
+  if (st != ST_OK) return st;
+  p->vec = p->args.t.kind == KIND_ROWS ? p->args.t.vec : 1;
+  if (p->args.t.kind == KIND_ROWS && p->vec > 1) {
+    // same problem without vector accesses, for pointers that are not
+    // aligned to the planned vector
+    TileParams sp = params;
+    sp.max_vec_bytes = elem_bytes(p->args.p.dtype);
+    st = choose_tile(p->args.p, sp, &p->tile_scalar);
+    if (st != ST_OK) return st;
+  } else {
+    p->tile_scalar = p->args.t;
+  }
+  // grid: resident CTAs on every SM, capped by the tile count
+  auto size_grid = [&](const HpttTile &t, int vec, int *grid) -> int {
+    HpttArgs a = p->args;
+    a.t = t;
+    int per_sm = 0;
+    if (occupancy(a, vec, &per_sm) != cudaSuccess || per_sm < 1) return ST_CUDA;
+    if (params.ctas_per_sm > 0 && params.ctas_per_sm < per_sm) per_sm = params.ctas_per_sm;
+    int64_t g = static_cast<int64_t>(per_sm) * p->sm_count;
+    if (g > t.num_tiles) g = t.num_tiles;
+    if (g < 1) g = 1;
+    *grid = static_cast<int>(g);
+    return ST_OK;
+  };
+  st = size_grid(p->args.t, p->vec, &p->grid);
+  if (st != ST_OK) return st;
+  return size_grid(p->tile_scalar, 1, &p->grid_scalar);
+}
+
+int plan_vec_for_ptrs(const Plan *p) {
+  if (p->vec <= 1) return 1;
+  const uintptr_t bytes = static_cast<uintptr_t>(p->vec) * elem_bytes(p->args.p.dtype);
+  const uintptr_t a = reinterpret_cast<uintptr_t>(p->args.A);
+  const uintptr_t b = reinterpret_cast<uintptr_t>(p->args.B);
+  return (a % bytes == 0 && b % bytes == 0) ? p->vec : 1;
+}
+
+int plan_enqueue(Plan *p, cudaStream_t stream) {
+  if (!p->args.A || !p->args.B) return ST_NULL_DATA;
+  const int vec = plan_vec_for_ptrs(p);
+  cudaError_t e;
+  if (vec == p->vec) {
+    e = launch_single(p->args, vec, p->grid, stream);
+  } else {
+    HpttArgs a = p->args;
+    a.t = p->tile_scalar;
+    e = launch_single(a, 1, p->grid_scalar, stream);
+  }
+  return e == cudaSuccess ? ST_OK : ST_CUDA;
+}
+
+}  // namespace hptt_b200
+
+using namespace hptt_b200;
+
+extern "C" {
+
+int hptt_cuda_plan_create(int dtype, uint32_t rank, const uint32_t *in_size,
+                          const uint32_t *perm, const uint32_t *in_outer,
+                          const uint32_t *out_outer, const double *alpha,
+                          const double *beta, int complex_scalars,
+                          const void *in, void *out, uint32_t num_threads,
+                          double tuning_timeout, hptt_cuda_plan_t *plan) {
+  (void)num_threads;
+  if (!plan) return HPTT_ERR_HANDLE;
+  *plan = nullptr;
+  // argument guard in the reference's order (src/hptt.cc:25-56)
+  if (!in || !out) return HPTT_ERR_NULL_DATA;
+  if (elem_bytes(dtype) == 0) return HPTT_ERR_DTYPE;
+  int st = validate(static_cast<int>(rank), in_size, perm, in_outer, out_outer,
+                    in_outer ? static_cast<int>(rank) : 0,
+                    out_outer ? static_cast<int>(rank) : 0);
+  if (st != ST_OK) return st;
+  if (!alpha || !beta) return HPTT_ERR_SIZE_VALUE;
+
+  Plan *p = new (std::nothrow) Plan();
+  if (!p) return HPTT_ERR_ALLOC;
+  st = fuse(dtype, static_cast<int>(rank), in_size, perm, in_outer, out_outer, &p->args.p);
+  if (st != ST_OK) {
+    delete p;
+    return st;
+  }
+  p->elements = 1;
+  for (uint32_t d = 0; d < rank; ++d) p->elements *= in_size[d];
+  p->args.A = in;
+  p->args.B = out;
+  set_scalars(&p->args, alpha, beta, complex_scalars);
+  if (cudaGetDevice(&p->device) != cudaSuccess ||
+      cudaDeviceGetAttribute(&p->sm_count, cudaDevAttrMultiProcessorCount, p->device) !=
+          cudaSuccess) {
+    delete p;
+    return HPTT_ERR_NO_DEVICE;
+  }
+  TileParams params;
+  bool have = false;
+  if (tuning_timeout != 0.0) {
+    st = autotune(p, tuning_timeout, &params);
+    have = (st == ST_OK);
+  } else {
+    have = autotune_cache_lookup(p, &params);
+  }
+  if (!have) params = TileParams();
+  st = plan_tiles(p, params);
+  if (st != ST_OK && have) st = plan_tiles(p, TileParams());
+  if (st != ST_OK) {
+    delete p;
+    return st;
+  }
+  *plan = reinterpret_cast<hptt_cuda_plan_t>(p);
+  return HPTT_OK;
+}
+
+int hptt_cuda_plan_exec(hptt_cuda_plan_t plan) {
+  Plan *p = reinterpret_cast<Plan *>(plan);
+  if (!plan_valid(p)) return HPTT_ERR_HANDLE;
+  return plan_enqueue(p, p->stream);
+}
+
+int hptt_cuda_plan_exec_on(hptt_cuda_plan_t plan, void *stream) {
+  Plan *p = reinterpret_cast<Plan *>(plan);
+  if (!plan_valid(p)) return HPTT_ERR_HANDLE;
+  return plan_enqueue(p, static_cast<cudaStream_t>(stream));
+}
+
+int hptt_cuda_plan_reset_data(hptt_cuda_plan_t plan, const void *in, void *out) {
+  Plan *p = reinterpret_cast<Plan *>(plan);
+  if (!plan_valid(p)) return HPTT_ERR_HANDLE;
+  p->args.A = in;
+  p->args.B = out;
+  return HPTT_OK;
+}
+
+int hptt_cuda_plan_describe(hptt_cuda_plan_t plan, char *buf, size_t len) {
+  Plan *p = reinterpret_cast<Plan *>(plan);
+  if (!plan_valid(p)) return HPTT_ERR_HANDLE;
+  std::string s = describe(p->args.p, p->args.t);
+  char line[160];
+  std::snprintf(line, sizeof(line), "grid: %d CTAs on %d SMs%s\n", p->grid, p->sm_count,
+                p->tuned ? " (autotuned)" : "");
+  s += line;
+  if (buf && len) {
+    std::strncpy(buf, s.c_str(), len - 1);
+    buf[len - 1] = '\0';
+  }
+  return HPTT_OK;
+}
+
+int hptt_cuda_plan_set_thread_ids(hptt_cuda_plan_t plan, const int32_t *, uint32_t) {
+  return plan_valid(reinterpret_cast<Plan *>(plan)) ? HPTT_OK : HPTT_ERR_HANDLE;
+}
+
+int hptt_cuda_plan_unset_thread_ids(hptt_cuda_plan_t plan) {
+  return plan_valid(reinterpret_cast<Plan *>(plan)) ? HPTT_OK : HPTT_ERR_HANDLE;
+}
+
+int hptt_cuda_plan_set_stream(hptt_cuda_plan_t plan, void *stream) {
+  Plan *p = reinterpret_cast<Plan *>(plan);
+  if (!plan_valid(p)) return HPTT_ERR_HANDLE;
+  p->stream = static_cast<cudaStream_t>(stream);
+  return HPTT_OK;
+}
+
+int hptt_cuda_plan_sync(hptt_cuda_plan_t plan) {
+  Plan *p = reinterpret_cast<Plan *>(plan);
+  if (!plan_valid(p)) return HPTT_ERR_HANDLE;
+  return cudaStreamSynchronize(p->stream) == cudaSuccess ? HPTT_OK : HPTT_ERR_CUDA;
+}
+
+int hptt_cuda_plan_set_coef(hptt_cuda_plan_t plan, const double *alpha,
+                            const double *beta, int complex_scalars) {
+  Plan *p = reinterpret_cast<Plan *>(plan);
+  if (!plan_valid(p)) return HPTT_ERR_HANDLE;
+  if (!alpha || !beta) return HPTT_ERR_SIZE_VALUE;
+  set_scalars(&p->args, alpha, beta, complex_scalars);
+  return HPTT_OK;
+}
+
+int hptt_cuda_plan_bytes(hptt_cuda_plan_t plan, uint64_t *bytes) {
+  Plan *p = reinterpret_cast<Plan *>(plan);
+  if (!plan_valid(p) || !bytes) return HPTT_ERR_HANDLE;
+  const uint64_t sz = static_cast<uint64_t>(elem_bytes(p->args.p.dtype));
+  *bytes = p->elements * sz * (p->args.update ? 3u : 2u);
+  return HPTT_OK;
+}
+
+int hptt_cuda_plan_launches(hptt_cuda_plan_t plan, uint32_t *launches) {
+  Plan *p = reinterpret_cast<Plan *>(plan);
+  if (!plan_valid(p) || !launches) return HPTT_ERR_HANDLE;
+  *launches = p->args.t.num_tiles ? 1u : 0u;
+  return HPTT_OK;
+}
+
+int hptt_cuda_plan_destroy(hptt_cuda_plan_t plan) {
+  Plan *p = reinterpret_cast<Plan *>(plan);
+  if (!plan_valid(p)) return HPTT_ERR_HANDLE;
+  p->magic = 0;
+  delete p;
+  return HPTT_OK;
+}
+
+int hptt_cuda_plan_inspect(int dtype, uint32_t rank, const uint32_t *in_size,
+                           const uint32_t *perm, const uint32_t *in_outer,
+                           const uint32_t *out_outer, char *buf, size_t len) {
+  if (elem_bytes(dtype) == 0) return HPTT_ERR_DTYPE;
+  int st = validate(static_cast<int>(rank), in_size, perm, in_outer, out_outer,
+                    in_outer ? static_cast<int>(rank) : 0,
+                    out_outer ? static_cast<int>(rank) : 0);
+  if (st != ST_OK) return st;
+  HpttProblem p;
+  st = fuse(dtype, static_cast<int>(rank), in_size, perm, in_outer, out_outer, &p);
+  if (st != ST_OK) return st;
+  HpttTile t;
+  st = choose_tile(p, TileParams(), &t);
+  if (st != ST_OK) return st;
+  const std::string s = describe(p, t);
+  if (buf && len) {
+    std::strncpy(buf, s.c_str(), len - 1);
+    buf[len - 1] = '\0';
+  }
+  return HPTT_OK;
+}
+
+const char *hptt_cuda_status_string(int status) { return status_string(status); }
+
+const char *hptt_cuda_version(void) { return "hptt-b200 0.1 (sm_100a)"; }
+
+}  // extern "C"

@@ -74,6 +74,20 @@ struct HpttTile {
   int32_t smem_bytes;         // dynamic shared memory for one CTA
 };
 
+// Per-thread iterations of one phase, sized so every thread keeps about 64
+// (tile) or 128 (rows) bytes of loads in flight without spilling.
+#ifdef __CUDACC__
+#define HPTT_HD __host__ __device__
+#else
+#define HPTT_HD
+#endif
+HPTT_HD constexpr int hptt_jmax_tile(int elem_bytes) {
+  return elem_bytes >= 16 ? 4 : (elem_bytes >= 8 ? 8 : 16);
+}
+HPTT_HD constexpr int hptt_jmax_rows(int access_bytes) {
+  return access_bytes >= 16 ? 8 : 16;
+}
+
 // Everything one launch (or one batch entry) needs.
 struct HpttArgs {
   HpttProblem p;

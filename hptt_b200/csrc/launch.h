@@ -1,0 +1,24 @@
+// Host-side entry points into the CUDA kernels.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "desc.h"
+
+namespace hptt_b200 {
+
+// Kernel function for these arguments; vec = elements per access for
+// KIND_ROWS (1 when the pointers are not aligned for the planned vector).
+const void *kernel_for(const HpttArgs &a, int vec);
+
+// Threads per CTA the kernels are compiled for.
+int kernel_threads();
+
+// Enqueue one transpose.  `grid` CTAs loop over the tiles.
+cudaError_t launch_single(const HpttArgs &a, int vec, int grid, cudaStream_t stream);
+
+// Resident CTAs per SM for this launch shape (also raises the dynamic
+// shared-memory limit of the kernel when needed).
+cudaError_t occupancy(const HpttArgs &a, int vec, int *ctas_per_sm);
+
+}  // namespace hptt_b200

@@ -1,0 +1,45 @@
+// Plan object behind the C ABI.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+
+#include "desc.h"
+#include "planner.h"
+
+namespace hptt_b200 {
+
+constexpr uint32_t kPlanMagic = 0x48505454u;  // "HPTT"
+
+struct Plan {
+  uint32_t magic = kPlanMagic;
+  HpttArgs args{};          // fused problem, vector tile, scalars, pointers
+  HpttTile tile_scalar{};   // same problem without vector accesses
+  int vec = 1;              // planned elements per access (KIND_ROWS)
+  int grid = 0, grid_scalar = 0;
+  int device = 0;
+  int sm_count = 0;
+  cudaStream_t stream = nullptr;
+  uint64_t elements = 0;    // N = prod(in_size)
+  TileParams params;        // chosen by heuristic or tuner
+  bool tuned = false;
+};
+
+// Fill scalars/mode/update from alpha, beta.
+void set_scalars(HpttArgs *a, const double *alpha, const double *beta,
+                 int complex_scalars);
+
+// Plan the tile for `params` and size the grid.  Needs a current device.
+int plan_tiles(Plan *p, const TileParams &params);
+
+// Enqueue one exec of the plan on `stream`.
+int plan_enqueue(Plan *p, cudaStream_t stream);
+
+// The effective vector width and tile for the current pointers.
+int plan_vec_for_ptrs(const Plan *p);
+
+bool plan_valid(const Plan *p);
+
+}  // namespace hptt_b200

@@ -1,0 +1,545 @@
+// Host planner: argument guard, index fusion, tile and grid selection.
+//
+// This replaces the reference's CPU planning layer
+//   - argument guard            src/hptt.cc:25-56
+//   - index fusion              inc/hptt/param/parameter_trans.tcc:223-283, 65-97
+//   - loop-order / thread split inc/hptt/plan/plan_trans_util.tcc (whole file)
+// with a GPU tile and grid chooser.  The fusion rule is the reference's
+// (adjacent-and-in-order under perm, unpadded) stated on strides: two
+// neighbouring output dims fuse when they are consecutive input dims and the
+// upper one's stride equals the lower one's stride times its extent in both
+// A and B.  Extent-1 dims are dropped first (they never change an offset).
+#include "planner.h"
+
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <sstream>
+#include <vector>
+
+namespace hptt_b200 {
+
+
+const char *status_string(int st) {
+  switch (st) {
+    case ST_OK: return "ok";
+    case ST_NULL_DATA: return "null data pointer";
+    case ST_BAD_RANK: return "tensor rank must be >= 2 (and <= 8)";
+    case ST_BAD_SIZE_VECTOR: return "size vector length does not match the rank";
+    case ST_BAD_SIZE_VALUE: return "zero extent or outer size below inner size";
+    case ST_BAD_PERM: return "perm is not a permutation of 0..rank-1";
+    case ST_BAD_DTYPE: return "unknown element type";
+    case ST_CUDA: return "CUDA runtime error";
+    case ST_NO_DEVICE: return "no CUDA device";
+    case ST_ALLOC: return "allocation failed";
+    case ST_BUDGET: return "request exceeds the memory budget";
+    case ST_BAD_HANDLE: return "invalid handle";
+    case ST_TIMEOUT: return "bounded wait ran out";
+    case ST_TOO_LARGE: return "size beyond what this build supports";
+    case ST_BUSY: return "no free slot";
+    default: return "unknown status";
+  }
+}
+
+int elem_bytes(int dtype) {
+  switch (dtype) {
+    case DT_F32: return 4;
+    case DT_F64: return 8;
+    case DT_C64: return 8;
+    case DT_C128: return 16;
+    default: return 0;
+  }
+}
+
+int validate(int rank, const uint32_t *in_size, const uint32_t *perm,
+             const uint32_t *in_outer, const uint32_t *out_outer,
+             int in_outer_len, int out_outer_len) {
+  // Order checks follow src/hptt.cc:30-56.  The permutation is validated
+  // before it is used as an index (the reference reads out_outer[perm[i]]
+  // first); both orders reject the same inputs.
+  if (rank <= 1) return ST_BAD_RANK;
+  if (rank > HPTT_MAX_RANK) return ST_BAD_RANK;
+  if (!in_size || !perm) return ST_BAD_SIZE_VECTOR;
+  if ((in_outer_len != 0 && in_outer_len != rank) ||
+      (out_outer_len != 0 && out_outer_len != rank))
+    return ST_BAD_SIZE_VECTOR;
+  if ((in_outer_len != 0 && !in_outer) || (out_outer_len != 0 && !out_outer))
+    return ST_BAD_SIZE_VECTOR;
+  bool seen[HPTT_MAX_RANK] = {false};
+  bool perm_ok = true;
+  for (int k = 0; k < rank; ++k) {
+    if (perm[k] >= static_cast<uint32_t>(rank) || seen[perm[k]]) {
+      perm_ok = false;
+      break;
+    }
+    seen[perm[k]] = true;
+  }
+  if (perm_ok) {
+    for (int i = 0; i < rank; ++i) {
+      if (in_size[i] == 0) return ST_BAD_SIZE_VALUE;
+      if (in_outer_len && in_outer[i] < in_size[i]) return ST_BAD_SIZE_VALUE;
+      // reference check, src/hptt.cc:47-49
+      if (out_outer_len && out_outer[perm[i]] < in_size[i]) return ST_BAD_SIZE_VALUE;
+    }
+    // memory-safety check the reference omits: output dim k has extent
+    // in_size[perm[k]] (hptt_trans_gen.py:196-197).
+    if (out_outer_len)
+      for (int k = 0; k < rank; ++k)
+        if (out_outer[k] < in_size[perm[k]]) return ST_BAD_SIZE_VALUE;
+    return ST_OK;
+  }
+  for (int i = 0; i < rank; ++i)
+    if (in_size[i] == 0) return ST_BAD_SIZE_VALUE;
+  return ST_BAD_PERM;
+}
+
+int fuse(int dtype, int rank, const uint32_t *in_size, const uint32_t *perm,
+         const uint32_t *in_outer, const uint32_t *out_outer,
+         HpttProblem *out) {
+  if (elem_bytes(dtype) == 0) return ST_BAD_DTYPE;
+  int64_t n[HPTT_MAX_RANK], sA[HPTT_MAX_RANK], sB[HPTT_MAX_RANK];
+  int q[HPTT_MAX_RANK];
+  int64_t s = 1;
+  for (int d = 0; d < rank; ++d) {
+    n[d] = in_size[d];
+    sA[d] = s;
+    s *= in_outer ? in_outer[d] : in_size[d];
+  }
+  s = 1;
+  int64_t sBout[HPTT_MAX_RANK];
+  for (int k = 0; k < rank; ++k) {
+    q[perm[k]] = k;
+    sBout[k] = s;
+    s *= out_outer ? out_outer[k] : in_size[perm[k]];
+  }
+  for (int d = 0; d < rank; ++d) sB[d] = sBout[q[d]];
+
+  // Input dims in output order, extent-1 dims dropped.
+  std::vector<int> ord;
+  for (int k = 0; k < rank; ++k)
+    if (n[perm[k]] > 1) ord.push_back(static_cast<int>(perm[k]));
+
+  std::memset(out, 0, sizeof(*out));
+  out->dtype = dtype;
+  if (ord.empty()) {  // a single element
+    out->rank = 1;
+    out->n[0] = 1;
+    out->sA[0] = 1;
+    out->sB[0] = 1;
+    out->perm[0] = 0;
+    return ST_OK;
+  }
+  // next kept input dim after d (input order)
+  auto next_kept = [&](int d) {
+    for (int e = d + 1; e < rank; ++e)
+      if (n[e] > 1) return e;
+    return -1;
+  };
+  struct Group { int first, last; int64_t ext; };
+  std::vector<Group> groups;  // in output order
+  for (int d : ord) {
+    if (!groups.empty()) {
+      Group &g = groups.back();
+      const int prev = g.last;
+      if (next_kept(prev) == d && sA[d] == sA[prev] * n[prev] &&
+          sB[d] == sB[prev] * n[prev]) {
+        g.last = d;
+        g.ext *= n[d];
+        continue;
+      }
+    }
+    groups.push_back({d, d, n[d]});
+  }
+  // groups sorted by first input dim -> fused input dims
+  std::vector<int> by_in(groups.size());
+  for (size_t i = 0; i < groups.size(); ++i) by_in[i] = static_cast<int>(i);
+  std::sort(by_in.begin(), by_in.end(), [&](int a, int b) {
+    return groups[a].first < groups[b].first;
+  });
+  std::vector<int> id_of_group(groups.size());
+  out->rank = static_cast<int32_t>(groups.size());
+  for (size_t i = 0; i < by_in.size(); ++i) {
+    const Group &g = groups[by_in[i]];
+    id_of_group[by_in[i]] = static_cast<int>(i);
+    out->n[i] = g.ext;
+    out->sA[i] = sA[g.first];
+    out->sB[i] = sB[g.first];
+  }
+  for (size_t k = 0; k < groups.size(); ++k) out->perm[k] = id_of_group[k];
+  return ST_OK;
+}
+
+namespace {
+
+int64_t cdiv(int64_t a, int64_t b) { return (a + b - 1) / b; }
+
+// Shared-memory wavefronts for one warp whose lanes access byte addresses
+// addr[lane] (each lane `bytes` wide); returns wavefronts beyond the ideal.
+int excess_wavefronts(const int64_t *addr, int lanes, int bytes) {
+  // count distinct 4-byte words per bank
+  std::vector<int64_t> words[32];
+  for (int l = 0; l < lanes; ++l) {
+    if (addr[l] < 0) continue;
+    for (int b = 0; b < bytes; b += 4) {
+      const int64_t w = (addr[l] + b) / 4;
+      auto &v = words[w % 32];
+      if (std::find(v.begin(), v.end(), w) == v.end()) v.push_back(w);
+    }
+  }
+  size_t worst = 0;
+  int active = 0;
+  for (int l = 0; l < lanes; ++l) active += addr[l] >= 0;
+  for (auto &v : words) worst = std::max(worst, v.size());
+  const int ideal = static_cast<int>(cdiv(static_cast<int64_t>(active) * bytes, 128));
+  return static_cast<int>(worst) - std::max(ideal, 1);
+}
+
+int bank_cost(const HpttTile &t, int ld, int sz) {
+  int cost = 0;
+  int64_t addr[32];
+  const int warps = std::min(t.nt / 32, 4);
+  for (int w = 0; w < warps; ++w) {
+    // load phase: thread -> (e, y0), element at y*LD + e
+    for (int l = 0; l < 32; ++l) {
+      const int tid = w * 32 + l;
+      if (tid < t.R1 * t.RW) {
+        const int e = tid % t.RW, y = tid / t.RW;
+        addr[l] = (y < t.TY) ? static_cast<int64_t>(y * ld + e) * sz : -1;
+      } else {
+        addr[l] = -1;
+      }
+    }
+    cost += excess_wavefronts(addr, 32, sz);
+    // store phase: thread -> (e2, x0); e2 = w + W*y; element at y*LD + w + W*x
+    for (int l = 0; l < 32; ++l) {
+      const int tid = w * 32 + l;
+      if (tid < t.R2 * t.WTY) {
+        const int e2 = tid % t.WTY, x = tid / t.WTY;
+        const int ww = e2 % t.W, y = e2 / t.W;
+        addr[l] = (x < t.TX) ? static_cast<int64_t>(y * ld + ww + t.W * x) * sz : -1;
+      } else {
+        addr[l] = -1;
+      }
+    }
+    cost += excess_wavefronts(addr, 32, sz);
+  }
+  return cost;
+}
+
+struct Side {
+  std::vector<int> d;
+  std::vector<int64_t> t;
+  int64_t prod() const {
+    int64_t p = 1;
+    for (auto v : t) p *= v;
+    return p;
+  }
+};
+
+bool shape_ok(const TileParams &tp, int64_t W, const Side &X, const Side &Y,
+              int sz) {
+  const int kJMax = hptt_jmax_tile(sz);
+  const int64_t TX = X.prod(), TY = Y.prod();
+  const int64_t RW = W * TX, WTY = W * TY;
+  if (RW > tp.nt || WTY > tp.nt) return false;
+  const int64_t R1 = tp.nt / RW, R2 = tp.nt / WTY;
+  if (cdiv(TY, R1) > kJMax || cdiv(TX, R2) > kJMax) return false;
+  if ((RW + 31) * TY * sz > tp.smem_bytes + 32 * TY * sz) return false;
+  return true;
+}
+
+void finish_grid(const HpttProblem &p, HpttTile *t, const int64_t *tile_ext,
+                 const std::vector<int> &chunk_first) {
+  // grid dims: chunked tile dims first, then every dim not fully inside the
+  // tile in input order
+  t->ng = 0;
+  bool used[HPTT_MAX_RANK] = {false};
+  uint64_t tiles = 1;
+  auto add = [&](int d) {
+    const int64_t cnt = cdiv(p.n[d], tile_ext[d]);
+    used[d] = true;
+    if (cnt <= 1) return;
+    t->gd[t->ng] = d;
+    t->gcnt[t->ng] = static_cast<uint32_t>(cnt);
+    t->gstep[t->ng] = static_cast<int32_t>(tile_ext[d]);
+    ++t->ng;
+    tiles *= static_cast<uint64_t>(cnt);
+  };
+  for (int d : chunk_first)
+    if (d >= 0 && !used[d]) add(d);
+  for (int d = 0; d < p.rank; ++d)
+    if (!used[d]) add(d);
+  t->num_tiles = tiles > 0x7fffffffULL ? 0 : static_cast<uint32_t>(tiles);
+}
+
+int choose_rows(const HpttProblem &p, const TileParams &tp, HpttTile *t) {
+  const int sz = elem_bytes(p.dtype);
+  std::memset(t, 0, sizeof(*t));
+  t->kind = KIND_ROWS;
+  t->nt = tp.nt;
+  t->xc = t->yc = t->wc = -1;
+  const int64_t n0 = p.n[0];
+  // widest vector (<= 16 bytes) that divides the row and every other stride
+  int vec = std::max(1, std::min(16, tp.max_vec_bytes) / sz);
+  while (vec > 1) {
+    bool ok = (n0 % vec == 0) && p.sA[0] == 1 && p.sB[0] == 1;
+    for (int d = 1; d < p.rank && ok; ++d)
+      ok = (p.sA[d] % vec == 0) && (p.sB[d] % vec == 0);
+    if (ok) break;
+    vec /= 2;
+  }
+  t->vec = vec;
+  const int64_t nvec_row = n0 / vec;
+  int64_t wv = std::min<int64_t>(nvec_row, tp.nt);  // vectors per tile row
+  t->W = static_cast<int32_t>(wv * vec);
+  if (t->W < n0) t->wc = 0;
+  t->RW = static_cast<int32_t>(wv);  // threads along a row
+  t->R1 = static_cast<int32_t>(tp.nt / wv);
+  const int kJMax = hptt_jmax_rows(vec * sz);
+  // rows: other dims in output order, full then chunked, up to the volume
+  const int64_t rows_target = std::max<int64_t>(
+      1, std::min<int64_t>(static_cast<int64_t>(t->R1) * kJMax,
+                           cdiv(tp.vmin_bytes, static_cast<int64_t>(t->W) * sz)));
+  int64_t TY = 1;
+  int64_t tile_ext[HPTT_MAX_RANK];
+  for (int d = 0; d < p.rank; ++d) tile_ext[d] = 1;
+  tile_ext[0] = t->W;
+  for (int k = 1; k < p.rank && TY < rows_target; ++k) {
+    const int d = p.perm[k];
+    const int64_t tt = std::min<int64_t>(p.n[d], rows_target / TY);
+    if (tt <= 1) break;
+    t->yd[t->ny] = d;
+    t->yt[t->ny] = static_cast<int32_t>(tt);
+    ++t->ny;
+    tile_ext[d] = tt;
+    TY *= tt;
+    if (tt < p.n[d]) {
+      t->yc = d;
+      break;
+    }
+  }
+  t->TY = static_cast<int32_t>(TY);
+  t->TX = 1;
+  t->J1 = static_cast<int32_t>(cdiv(TY, t->R1));
+  t->WTY = t->W;
+  t->LD = 0;
+  finish_grid(p, t, tile_ext, {t->wc, t->yc});
+  // in-tile offsets
+  int64_t maxA = (t->W - 1) * p.sA[0], maxB = (t->W - 1) * p.sB[0];
+  for (int i = 0; i < t->ny; ++i) {
+    maxA += (t->yt[i] - 1) * p.sA[t->yd[i]];
+    maxB += (t->yt[i] - 1) * p.sB[t->yd[i]];
+  }
+  t->big_offsets = (maxA >= 0x7fffffffLL || maxB >= 0x7fffffffLL);
+  const int off = t->big_offsets ? 8 : 4;
+  t->smem_bytes = static_cast<int32_t>(TY * (2 * off + 4));
+  return t->num_tiles ? ST_OK : ST_TOO_LARGE;
+}
+
+}  // namespace
+
+int choose_tile(const HpttProblem &p, const TileParams &tp, HpttTile *t) {
+  const int sz = elem_bytes(p.dtype);
+  const int r = p.rank;
+  const bool common = p.perm[0] == 0;
+  if (r == 1 || (common && p.n[0] * sz >= tp.rows_min_bytes))
+    return choose_rows(p, tp, t);
+  if (common && p.n[0] > tp.nt / 2) return choose_rows(p, tp, t);
+
+  std::memset(t, 0, sizeof(*t));
+  t->kind = KIND_TILE;
+  t->nt = tp.nt;
+  t->vec = 1;
+  t->xc = t->yc = t->wc = -1;
+  const int64_t W = common ? p.n[0] : 1;
+  const int si = common ? 1 : 0, so = common ? 1 : 0;
+  const int64_t target = std::max<int64_t>(4, tp.run_bytes / sz);
+  bool in_tile[HPTT_MAX_RANK] = {false};
+  if (common) in_tile[0] = true;
+
+  Side X, Y;
+  {
+    int64_t prod = W;
+    for (int d = si; d < r; ++d) {
+      if (d == p.perm[so]) break;
+      const int64_t cap = tp.nt / prod;
+      const int64_t tt = std::min({p.n[d], cdiv(target, prod), cap});
+      if (tt < 1) break;
+      X.d.push_back(d);
+      X.t.push_back(tt);
+      in_tile[d] = true;
+      prod *= tt;
+      if (tt < p.n[d] || prod >= target) break;
+    }
+    prod = W;
+    for (int k = so; k < r; ++k) {
+      const int d = p.perm[k];
+      if (in_tile[d]) break;
+      const int64_t cap = tp.nt / prod;
+      const int64_t tt = std::min({p.n[d], cdiv(target, prod), cap});
+      if (tt < 1) break;
+      Y.d.push_back(d);
+      Y.t.push_back(tt);
+      in_tile[d] = true;
+      prod *= tt;
+      if (tt < p.n[d] || prod >= target) break;
+    }
+  }
+  // shrink until the shape fits the thread mapping (the larger side first)
+  for (int guard = 0; guard < 4096 && !shape_ok(tp, W, X, Y, sz); ++guard) {
+    Side *S = (X.prod() >= Y.prod()) ? &X : &Y;
+    if (S->d.empty()) S = (S == &X) ? &Y : &X;
+    if (S->d.empty()) break;
+    int64_t &tt = S->t.back();
+    if (tt > 1) {
+      tt = std::max<int64_t>(1, (tt * 3) / 4);
+    } else {
+      in_tile[S->d.back()] = false;
+      S->d.pop_back();
+      S->t.pop_back();
+    }
+  }
+  // grow the tile until it holds vmin bytes
+  const int64_t vmin = std::max<int64_t>(1, tp.vmin_bytes / sz);
+  auto vol = [&]() { return W * X.prod() * Y.prod(); };
+  auto next_in = [&](const Side &S, bool output_order) -> int {
+    // next dim to add after a full last dim
+    if (output_order) {
+      for (int k = so; k < r; ++k) {
+        const int d = p.perm[k];
+        if (!in_tile[d]) return d;
+      }
+      return -1;
+    }
+    for (int d = si; d < r; ++d)
+      if (!in_tile[d]) return d;
+    (void)S;
+    return -1;
+  };
+  for (int iter = 0; iter < 64 && vol() < vmin; ++iter) {
+    bool grown = false;
+    // the side with the shorter run first
+    const bool x_first = X.prod() <= Y.prod();
+    for (int pass = 0; pass < 4 && !grown; ++pass) {
+      const bool onX = (pass % 2 == 0) ? x_first : !x_first;
+      Side &S = onX ? X : Y;
+      if (pass < 2) {
+        // enlarge the chunked last dim
+        if (S.d.empty()) continue;
+        const int d = S.d.back();
+        int64_t &tt = S.t.back();
+        if (tt >= p.n[d]) continue;
+        const int64_t old = tt;
+        const int64_t want = std::min<int64_t>(p.n[d], std::max<int64_t>(old + 1, old * 2));
+        tt = want;
+        while (tt > old && !shape_ok(tp, W, X, Y, sz)) --tt;
+        if (tt > old) grown = true; else tt = old;
+      } else {
+        if (!S.d.empty() && S.t.back() < p.n[S.d.back()]) continue;
+        const int d = next_in(S, !onX);
+        if (d < 0) continue;
+        S.d.push_back(d);
+        S.t.push_back(1);
+        in_tile[d] = true;
+        int64_t &tt = S.t.back();
+        const int64_t want = std::min<int64_t>(p.n[d], cdiv(vmin, vol()));
+        tt = std::max<int64_t>(1, want);
+        while (tt > 1 && !shape_ok(tp, W, X, Y, sz)) --tt;
+        if (tt > 1 && shape_ok(tp, W, X, Y, sz)) {
+          grown = true;
+        } else {
+          S.d.pop_back();
+          S.t.pop_back();
+          in_tile[d] = false;
+        }
+      }
+    }
+    if (!grown) break;
+  }
+  if (!shape_ok(tp, W, X, Y, sz)) return ST_TOO_LARGE;
+
+  t->W = static_cast<int32_t>(W);
+  t->nx = static_cast<int32_t>(X.d.size());
+  t->ny = static_cast<int32_t>(Y.d.size());
+  int64_t tile_ext[HPTT_MAX_RANK];
+  for (int d = 0; d < r; ++d) tile_ext[d] = 1;
+  if (common) tile_ext[0] = W;
+  for (int i = 0; i < t->nx; ++i) {
+    t->xd[i] = X.d[i];
+    t->xt[i] = static_cast<int32_t>(X.t[i]);
+    tile_ext[X.d[i]] = X.t[i];
+  }
+  for (int i = 0; i < t->ny; ++i) {
+    t->yd[i] = Y.d[i];
+    t->yt[i] = static_cast<int32_t>(Y.t[i]);
+    tile_ext[Y.d[i]] = Y.t[i];
+  }
+  if (t->nx && X.t.back() < p.n[X.d.back()]) t->xc = X.d.back();
+  if (t->ny && Y.t.back() < p.n[Y.d.back()]) t->yc = Y.d.back();
+  t->TX = static_cast<int32_t>(X.prod());
+  t->TY = static_cast<int32_t>(Y.prod());
+  t->RW = static_cast<int32_t>(W * t->TX);
+  t->WTY = static_cast<int32_t>(W * t->TY);
+  t->R1 = t->nt / t->RW;
+  t->J1 = static_cast<int32_t>(cdiv(t->TY, t->R1));
+  t->R2 = t->nt / t->WTY;
+  t->J2 = static_cast<int32_t>(cdiv(t->TX, t->R2));
+  // row pitch with the fewest shared-memory bank conflicts
+  int best_ld = t->RW, best_cost = 1 << 30;
+  const int span = std::max(1, 128 / sz);
+  for (int ld = t->RW; ld < t->RW + span; ++ld) {
+    const int c = bank_cost(*t, ld, sz);
+    if (c < best_cost) {
+      best_cost = c;
+      best_ld = ld;
+    }
+    if (c == 0) break;
+  }
+  t->LD = best_ld;
+  finish_grid(p, t, tile_ext, {t->xc, t->yc});
+
+  int64_t maxA = 0, maxB = 0;
+  if (common) {
+    maxA += (W - 1) * p.sA[0];
+    maxB += (W - 1) * p.sB[0];
+  }
+  for (int i = 0; i < t->nx; ++i) {
+    maxA += (t->xt[i] - 1) * p.sA[t->xd[i]];
+    maxB += (t->xt[i] - 1) * p.sB[t->xd[i]];
+  }
+  for (int i = 0; i < t->ny; ++i) {
+    maxA += (t->yt[i] - 1) * p.sA[t->yd[i]];
+    maxB += (t->yt[i] - 1) * p.sB[t->yd[i]];
+  }
+  t->big_offsets = (maxA >= 0x7fffffffLL || maxB >= 0x7fffffffLL);
+  const int off = t->big_offsets ? 8 : 4;
+  const int64_t data = (static_cast<int64_t>(t->TY) * t->LD * sz + 15) / 16 * 16;
+  t->smem_bytes = static_cast<int32_t>(data + (t->TY + t->TX) * (off + 4));
+  return t->num_tiles ? ST_OK : ST_TOO_LARGE;
+}
+
+std::string describe(const HpttProblem &p, const HpttTile &t) {
+  static const char *names[] = {"float", "double", "complex float", "complex double"};
+  std::ostringstream os;
+  os << "dtype: " << names[p.dtype & 3] << "\n";
+  os << "fused rank: " << p.rank << "\n  extents (input order):";
+  for (int d = 0; d < p.rank; ++d) os << " " << p.n[d];
+  os << "\n  perm (output dim -> input dim):";
+  for (int k = 0; k < p.rank; ++k) os << " " << p.perm[k];
+  os << "\n  strides A:";
+  for (int d = 0; d < p.rank; ++d) os << " " << p.sA[d];
+  os << "\n  strides B:";
+  for (int d = 0; d < p.rank; ++d) os << " " << p.sB[d];
+  os << "\nkernel: " << (t.kind == KIND_TILE ? "tile (shared-memory transpose)" : "rows (shared stride-1)")
+     << ", " << t.nt << " threads/CTA";
+  if (t.kind == KIND_ROWS) os << ", vector " << t.vec;
+  os << "\n  tile W=" << t.W << " X{";
+  for (int i = 0; i < t.nx; ++i) os << (i ? "," : "") << t.xd[i] << ":" << t.xt[i];
+  os << "} Y{";
+  for (int i = 0; i < t.ny; ++i) os << (i ? "," : "") << t.yd[i] << ":" << t.yt[i];
+  os << "} TX=" << t.TX << " TY=" << t.TY << " LD=" << t.LD << "\n  tiles: " << t.num_tiles
+     << ", smem/CTA: " << t.smem_bytes << " B\n";
+  return os.str();
+}
+
+}  // namespace hptt_b200

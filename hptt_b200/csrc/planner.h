@@ -1,0 +1,62 @@
+// Host planner: argument guard, index fusion and tile/grid selection.
+#pragma once
+
+#include <stdint.h>
+#include <string>
+
+#include "desc.h"
+
+namespace hptt_b200 {
+
+// Status codes (mirrored in include/hptt_cuda.h).
+enum Status : int {
+  ST_OK = 0,
+  ST_NULL_DATA = 1,        // in or out pointer is null
+  ST_BAD_RANK = 2,         // rank < 2 (or above the supported maximum)
+  ST_BAD_SIZE_VECTOR = 3,  // a size vector has the wrong length
+  ST_BAD_SIZE_VALUE = 4,   // zero extent or outer size below inner size
+  ST_BAD_PERM = 5,         // perm is not a permutation
+  ST_BAD_DTYPE = 6,
+  ST_CUDA = 7,             // a CUDA runtime call failed
+  ST_NO_DEVICE = 8,
+  ST_ALLOC = 9,            // host or device allocation failed
+  ST_BUDGET = 10,          // request exceeds the memory budget
+  ST_BAD_HANDLE = 11,      // null or destroyed plan/batch/server
+  ST_TIMEOUT = 12,         // a bounded wait ran out
+  ST_TOO_LARGE = 13,       // a size beyond what this build supports
+  ST_BUSY = 14,            // no free slot (served form)
+};
+
+const char *status_string(int st);
+
+// Tuning knobs of the tile chooser; the autotuner searches over these.
+struct TileParams {
+  int nt = 256;            // threads per CTA
+  int run_bytes = 256;     // contiguous bytes wanted on each side of a tile
+  int vmin_bytes = 16384;  // grow tiles to at least this many bytes
+  int smem_bytes = 32768;  // data bytes one tile may hold in shared memory
+  int rows_min_bytes = 512;  // shared stride-1 run long enough for KIND_ROWS
+  int ctas_per_sm = 0;     // 0: as many as fit
+  int max_vec_bytes = 16;  // widest vector access (KIND_ROWS)
+};
+
+// Reference argument guard (src/hptt.cc:25-56) plus the one check the
+// reference omits for memory safety (out_outer[k] >= out_size[k]).
+int validate(int rank, const uint32_t *in_size, const uint32_t *perm,
+             const uint32_t *in_outer, const uint32_t *out_outer,
+             int in_outer_len, int out_outer_len);
+
+// Fuse index groups.  Output: problem in input-dim order with strides.
+int fuse(int dtype, int rank, const uint32_t *in_size, const uint32_t *perm,
+         const uint32_t *in_outer, const uint32_t *out_outer,
+         HpttProblem *out);
+
+// Choose tile and grid.  Returns ST_OK or ST_TOO_LARGE.
+int choose_tile(const HpttProblem &p, const TileParams &tp, HpttTile *t);
+
+int elem_bytes(int dtype);
+
+// Human-readable plan summary (print_plan()).
+std::string describe(const HpttProblem &p, const HpttTile &t);
+
+}  // namespace hptt_b200

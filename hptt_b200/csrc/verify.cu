@@ -1,0 +1,206 @@
+// Host emulation of the kernels' addressing, for CPU tests.
+//
+// Runs the planner, then replays every tile and every thread of the launch
+// with the same index helpers the kernels use (kernels.cuh, compiled for the
+// host here) and checks, without a GPU:
+//   - every A read and every B read/write is inside the caller's buffers,
+//   - every shared-memory access is inside the tile buffer and reads a slot
+//     the load phase of the same tile wrote,
+//   - the element stored to B[j] is the one loaded from A[i] with
+//     j = perm-mapped(i), and every inner element of B is written exactly
+//     once while the padding of B is never touched.
+#include <cstdint>
+#include <cstring>
+#include <vector>
+
+#include "../../include/hptt_cuda.h"
+#include "kernels.cuh"
+#include "planner.h"
+
+namespace hptt_b200 {
+namespace {
+
+using namespace dev;
+
+struct Layout {
+  int rank;
+  std::vector<int64_t> in_size, in_outer, out_outer, perm;
+  int64_t nA = 1, nB = 1;
+  std::vector<int64_t> sa, sbo;  // input strides; output strides per output dim
+};
+
+// A index -> expected B index, or -1 if the A index is padding.
+int64_t map_a_to_b(const Layout &L, int64_t ia) {
+  int64_t c[HPTT_MAX_RANK];
+  int64_t rem = ia;
+  for (int d = 0; d < L.rank; ++d) {
+    c[d] = rem % L.in_outer[d];
+    rem /= L.in_outer[d];
+    if (c[d] >= L.in_size[d]) return -1;
+  }
+  int64_t ib = 0;
+  for (int k = 0; k < L.rank; ++k) ib += c[L.perm[k]] * L.sbo[k];
+  return ib;
+}
+
+bool b_is_inner(const Layout &L, int64_t ib) {
+  int64_t rem = ib;
+  for (int k = 0; k < L.rank; ++k) {
+    const int64_t c = rem % L.out_outer[k];
+    rem /= L.out_outer[k];
+    if (c >= L.in_size[L.perm[k]]) return false;
+  }
+  return true;
+}
+
+template <typename OffT>
+int replay_tile(const HpttProblem &P, const HpttTile &T, const Layout &L,
+                std::vector<uint8_t> &writes, uint64_t *checked) {
+  std::vector<OffT> tInY(T.TY), tOutX(T.TX);
+  std::vector<int> tCy(T.TY), tCx(T.TX);
+  tile_tables<OffT>(P, T, tInY.data(), tCy.data(), tOutX.data(), tCx.data(), 0, 1);
+  std::vector<TileThread<OffT>> th(T.nt);
+  for (int t = 0; t < T.nt; ++t) th[t] = tile_thread<OffT>(P, T, t);
+  const int esz = elem_bytes(P.dtype);
+  const int J = hptt_jmax_tile(esz);
+  if (T.J1 > J || T.J2 > J) return 101;
+  const int64_t smem_elems = static_cast<int64_t>(T.TY) * T.LD;
+  if (align16(static_cast<int>(smem_elems * esz)) + (T.TY + T.TX) * (static_cast<int>(sizeof(OffT)) + 4) >
+      T.smem_bytes)
+    return 102;
+  std::vector<int64_t> slot(smem_elems);
+  for (uint32_t tile = 0; tile < T.num_tiles; ++tile) {
+    const TileOrigin o = tile_origin(P, T, tile);
+    std::fill(slot.begin(), slot.end(), -2);
+    for (int t = 0; t < T.nt; ++t) {
+      const TileThread<OffT> &s = th[t];
+      if (!s.ld_active) continue;
+      for (int j = 0; j < J; ++j) {
+        const int y = s.y0 + j * T.R1;
+        if (!(j < T.J1 && y < T.TY)) continue;
+        const int64_t si = static_cast<int64_t>(y) * T.LD + s.sme;
+        if (si < 0 || si >= smem_elems) return 103;
+        if (o.interior || (s.cxe < o.remX && tCy[y] < o.remY)) {
+          const int64_t ia = o.bA + static_cast<int64_t>(s.inE) + static_cast<int64_t>(tInY[y]);
+          if (ia < 0 || ia >= L.nA) return 104;
+          if (slot[si] != -2) return 105;  // two writers of one slot
+          slot[si] = ia;
+        } else {
+          if (slot[si] == -2) slot[si] = -1;  // written with an unused value
+        }
+      }
+    }
+    for (int t = 0; t < T.nt; ++t) {
+      const TileThread<OffT> &s = th[t];
+      if (!s.st_active) continue;
+      for (int j = 0; j < J; ++j) {
+        const int x = s.x0 + j * T.R2;
+        if (!(j < T.J2 && x < T.TX)) continue;
+        if (!(o.interior || (s.cye2 < o.remY && tCx[x] < o.remX))) continue;
+        const int64_t si = static_cast<int64_t>(s.sme2) + static_cast<int64_t>(x) * T.W;
+        if (si < 0 || si >= smem_elems) return 106;
+        const int64_t ia = slot[si];
+        if (ia < 0) return 107;  // reads a slot no valid load wrote
+        const int64_t ib = o.bB + static_cast<int64_t>(s.outE2) + static_cast<int64_t>(tOutX[x]);
+        if (ib < 0 || ib >= L.nB) return 108;
+        if (map_a_to_b(L, ia) != ib) return 109;
+        if (writes[ib] != 0) return 110;
+        writes[ib] = 1;
+        ++*checked;
+      }
+    }
+  }
+  return 0;
+}
+
+template <typename OffT>
+int replay_rows(const HpttProblem &P, const HpttTile &T, const Layout &L, int vec,
+                std::vector<uint8_t> &writes, uint64_t *checked) {
+  std::vector<OffT> tInY(T.TY), tOutY(T.TY);
+  std::vector<int> tCy(T.TY);
+  rows_tables<OffT>(P, T, tInY.data(), tOutY.data(), tCy.data(), 0, 1);
+  const int esz = elem_bytes(P.dtype);
+  const int J = hptt_jmax_rows(esz * vec);
+  if (T.J1 > J) return 201;
+  if (T.TY * (2 * static_cast<int>(sizeof(OffT)) + 4) > T.smem_bytes) return 202;
+  if (vec > 1 && (P.sA[0] != 1 || P.sB[0] != 1)) return 203;
+  for (uint32_t tile = 0; tile < T.num_tiles; ++tile) {
+    const TileOrigin o = tile_origin(P, T, tile);
+    for (int t = 0; t < T.nt; ++t) {
+      const RowThread<OffT> s = rows_thread<OffT>(T, t);
+      if (!s.active) continue;
+      const int64_t col = static_cast<int64_t>(s.e) * vec;
+      const bool col_ok = o.interior || col < o.remX;
+      for (int j = 0; j < J; ++j) {
+        const int y = s.y0 + j * T.R1;
+        if (!(j < T.J1 && y < T.TY && col_ok && (o.interior || tCy[y] < o.remY))) continue;
+        const int64_t a0 = o.bA + col * P.sA[0] + static_cast<int64_t>(tInY[y]);
+        const int64_t b0 = o.bB + col * P.sB[0] + static_cast<int64_t>(tOutY[y]);
+        if (vec > 1 && ((a0 % vec) != 0 || (b0 % vec) != 0)) return 204;
+        for (int k = 0; k < vec; ++k) {
+          const int64_t ia = a0 + k, ib = b0 + k;
+          if (ia < 0 || ia >= L.nA) return 205;
+          if (ib < 0 || ib >= L.nB) return 206;
+          if (map_a_to_b(L, ia) != ib) return 207;
+          if (writes[ib] != 0) return 208;
+          writes[ib] = 1;
+          ++*checked;
+        }
+      }
+    }
+  }
+  return 0;
+}
+
+}  // namespace
+}  // namespace hptt_b200
+
+using namespace hptt_b200;
+
+extern "C" int hptt_cuda_debug_check_indexing(int dtype, uint32_t rank, const uint32_t *in_size,
+                                              const uint32_t *perm, const uint32_t *in_outer,
+                                              const uint32_t *out_outer, int max_vec_bytes,
+                                              uint64_t *checked) {
+  if (elem_bytes(dtype) == 0) return HPTT_ERR_DTYPE;
+  int st = validate(static_cast<int>(rank), in_size, perm, in_outer, out_outer,
+                    in_outer ? static_cast<int>(rank) : 0, out_outer ? static_cast<int>(rank) : 0);
+  if (st != ST_OK) return st;
+  HpttProblem P;
+  st = fuse(dtype, static_cast<int>(rank), in_size, perm, in_outer, out_outer, &P);
+  if (st != ST_OK) return st;
+  TileParams tp;
+  if (max_vec_bytes > 0) tp.max_vec_bytes = max_vec_bytes;
+  HpttTile T;
+  st = choose_tile(P, tp, &T);
+  if (st != ST_OK) return st;
+  Layout L;
+  L.rank = static_cast<int>(rank);
+  for (uint32_t d = 0; d < rank; ++d) {
+    L.in_size.push_back(in_size[d]);
+    L.in_outer.push_back(in_outer ? in_outer[d] : in_size[d]);
+    L.perm.push_back(perm[d]);
+  }
+  for (uint32_t k = 0; k < rank; ++k)
+    L.out_outer.push_back(out_outer ? out_outer[k] : in_size[perm[k]]);
+  for (uint32_t d = 0; d < rank; ++d) L.nA *= L.in_outer[d];
+  int64_t s = 1;
+  for (uint32_t k = 0; k < rank; ++k) {
+    L.sbo.push_back(s);
+    s *= L.out_outer[k];
+  }
+  L.nB = s;
+  std::vector<uint8_t> writes(static_cast<size_t>(L.nB), 0);
+  uint64_t n = 0;
+  int rc;
+  if (T.kind == KIND_TILE)
+    rc = T.big_offsets ? replay_tile<int64_t>(P, T, L, writes, &n)
+                       : replay_tile<uint32_t>(P, T, L, writes, &n);
+  else
+    rc = T.big_offsets ? replay_rows<int64_t>(P, T, L, T.vec, writes, &n)
+                       : replay_rows<uint32_t>(P, T, L, T.vec, writes, &n);
+  if (rc != 0) return 1000 + rc;
+  for (int64_t ib = 0; ib < L.nB; ++ib)
+    if (static_cast<bool>(writes[ib]) != b_is_inner(L, ib)) return 1300;
+  if (checked) *checked = n;
+  return 0;
+}

@@ -1,0 +1,174 @@
+/*
+ * hptt_cuda.h -- C ABI of libhptt_cuda.so, the B200 (sm_100a) engine for
+ *
+ *     B[perm(i)] = alpha * A[i] + beta * B[perm(i)]
+ *
+ * Column-major tensors (dimension 0 has stride 1), output extents
+ * out_size[k] = in_size[perm[k]], element types float, double, complex float
+ * and complex double, ranks 2..8.  All data pointers are DEVICE pointers.
+ *
+ * Every entry point returns an int status (HPTT_OK = 0).  No entry point
+ * throws, and none takes a C++ or torch type.
+ *
+ * Each declaration names the reference interface it replaces (file:line in
+ * the reference project).
+ */
+#ifndef HPTT_CUDA_H_
+#define HPTT_CUDA_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Element types.  Reference: hptt::FloatComplex / DoubleComplex
+ * (inc/hptt/types.h:21-22) and the four explicit instantiations
+ * (inc/hptt/hptt.h:99-123). */
+enum hptt_cuda_dtype {
+  HPTT_CUDA_F32 = 0,
+  HPTT_CUDA_F64 = 1,
+  HPTT_CUDA_C64 = 2,  /* float _Complex, layout of float2  */
+  HPTT_CUDA_C128 = 3  /* double _Complex, layout of double2 */
+};
+
+/* Status codes.  The reference returns nullptr from create_plan for the
+ * argument errors 1-5 (inc/hptt/hptt.h:71-83, src/hptt.cc:25-56); here each
+ * cause has its own code. */
+enum hptt_cuda_status {
+  HPTT_OK = 0,
+  HPTT_ERR_NULL_DATA = 1,
+  HPTT_ERR_RANK = 2,
+  HPTT_ERR_SIZE_VECTOR = 3,
+  HPTT_ERR_SIZE_VALUE = 4,
+  HPTT_ERR_PERM = 5,
+  HPTT_ERR_DTYPE = 6,
+  HPTT_ERR_CUDA = 7,
+  HPTT_ERR_NO_DEVICE = 8,
+  HPTT_ERR_ALLOC = 9,
+  HPTT_ERR_BUDGET = 10,
+  HPTT_ERR_HANDLE = 11,
+  HPTT_ERR_TIMEOUT = 12,
+  HPTT_ERR_TOO_LARGE = 13,
+  HPTT_ERR_BUSY = 14
+};
+
+typedef struct hptt_cuda_plan_s *hptt_cuda_plan_t;
+
+/*
+ * Create a transpose plan.
+ * Replaces: hptt::create_plan<T> (inc/hptt/hptt.h:85-93, src/hptt.cc:16-93)
+ * and the per-type factories create_trans_plan_impl_{s,d,c,z}
+ * (inc/hptt/impl/hptt_trans_impl.h:81-103, src/impl/hptt_trans_impl_s.cc:8-20).
+ *
+ *   in_size[rank], perm[rank]   as in the reference; rank >= 2
+ *   in_outer / out_outer        outer (padded) sizes or NULL; out_outer is
+ *                               indexed by OUTPUT dimension
+ *                               (inc/hptt/hptt.h:58-61)
+ *   alpha, beta                 two doubles each (re, im).  With
+ *                               complex_scalars == 0 only [0] is used, as a
+ *                               real scalar (the reference's
+ *                               DeducedFloatType, inc/hptt/types.h:29-54);
+ *                               complex_scalars != 0 (complex types only)
+ *                               applies full complex scalars -- an
+ *                               extension the reference cannot express.
+ *   in, out                     device pointers; never freed by the plan
+ *   num_threads                 accepted and ignored (GPU launch shape is
+ *                               chosen by the planner)
+ *   tuning_timeout              0: heuristic only; != 0: time candidate tile
+ *                               shapes on scratch buffers (< 0 all of them,
+ *                               > 0 for at most that many seconds) and cache
+ *                               the winner (inc/hptt/hptt.h:48-57)
+ * B is read only when |beta| >= 1e-16 (inc/hptt/impl/hptt_trans_impl.h:75-78).
+ */
+int hptt_cuda_plan_create(int dtype, uint32_t rank, const uint32_t *in_size,
+                          const uint32_t *perm, const uint32_t *in_outer,
+                          const uint32_t *out_outer, const double *alpha,
+                          const double *beta, int complex_scalars,
+                          const void *in, void *out, uint32_t num_threads,
+                          double tuning_timeout, hptt_cuda_plan_t *plan);
+
+/* Enqueue the transpose on the plan's stream (asynchronous).
+ * Replaces: CGraphTransPackBase::exec() / operator()()
+ * (inc/hptt/impl/hptt_trans.h:26-27). */
+int hptt_cuda_plan_exec(hptt_cuda_plan_t plan);
+
+/* Same, on an explicit cudaStream_t (passed as void*). Extension. */
+int hptt_cuda_plan_exec_on(hptt_cuda_plan_t plan, void *stream);
+
+/* Swap the data pointers; sizes, perm, scalars and tile choice are kept.
+ * Replaces: CGraphTransPackBase::reset_data (inc/hptt/impl/hptt_trans.h:29,
+ * inc/hptt/cgraph/cgraph_trans.tcc:64-68).  Like the reference it does not
+ * re-validate; a null pointer is rejected at exec instead. */
+int hptt_cuda_plan_reset_data(hptt_cuda_plan_t plan, const void *in, void *out);
+
+/* Write a readable plan summary (NUL-terminated, truncated to len).
+ * Replaces: CGraphTransPackBase::print_plan (inc/hptt/impl/hptt_trans.h:28). */
+int hptt_cuda_plan_describe(hptt_cuda_plan_t plan, char *buf, size_t len);
+
+/* Accepted no-ops: there is no host thread team on the GPU path.
+ * Replaces: set_thread_ids / unset_thread_ids
+ * (inc/hptt/impl/hptt_trans.h:30-31, inc/hptt/cgraph/cgraph_trans.tcc:71-83). */
+int hptt_cuda_plan_set_thread_ids(hptt_cuda_plan_t plan, const int32_t *ids,
+                                  uint32_t count);
+int hptt_cuda_plan_unset_thread_ids(hptt_cuda_plan_t plan);
+
+/* Stream used by hptt_cuda_plan_exec (cudaStream_t as void*; NULL = the
+ * legacy default stream, the initial setting).  Extension. */
+int hptt_cuda_plan_set_stream(hptt_cuda_plan_t plan, void *stream);
+
+/* Wait for the plan's stream.  Extension (exec is asynchronous). */
+int hptt_cuda_plan_sync(hptt_cuda_plan_t plan);
+
+/* Scalars: change alpha/beta on an existing plan (re-decides whether B is
+ * read).  Reference: ParamTrans::set_coef
+ * (inc/hptt/param/parameter_trans.tcc:161-168), used by its tuner. */
+int hptt_cuda_plan_set_coef(hptt_cuda_plan_t plan, const double *alpha,
+                            const double *beta, int complex_scalars);
+
+/* Algorithmic bytes one exec moves: 2*N*sizeof(T), plus N*sizeof(T) when B
+ * is read.  Extension, for throughput reporting. */
+int hptt_cuda_plan_bytes(hptt_cuda_plan_t plan, uint64_t *bytes);
+
+/* Kernel launches one exec issues (1, or 0 for an empty problem). */
+int hptt_cuda_plan_launches(hptt_cuda_plan_t plan, uint32_t *launches);
+
+/* Destroy the plan (does not touch the user's buffers).
+ * Replaces: the shared_ptr deleter of the reference plan
+ * (inc/hptt/impl/hptt_trans.h:22, src/hptt.cc:86-92). */
+int hptt_cuda_plan_destroy(hptt_cuda_plan_t plan);
+
+/* Host-only dry run of create: argument guard, index fusion and tile choice,
+ * without a device or data pointers.  Writes the plan summary that
+ * hptt_cuda_plan_describe would print (minus the grid line).  Extension, for
+ * tests and tooling.  Reference counterpart: the same guard
+ * (src/hptt.cc:25-56) and ParamTrans::merge_idx_
+ * (inc/hptt/param/parameter_trans.tcc:223-283). */
+int hptt_cuda_plan_inspect(int dtype, uint32_t rank, const uint32_t *in_size,
+                           const uint32_t *perm, const uint32_t *in_outer,
+                           const uint32_t *out_outer, char *buf, size_t len);
+
+/* Host-only replay of a launch's addressing: plans the problem, then walks
+ * every tile and thread with the kernels' own index helpers and checks that
+ * every access stays inside the buffers and shared memory, and that every
+ * inner element of B is written exactly once with the element of A the
+ * permutation maps to it.  max_vec_bytes limits vector accesses (0 = widest).
+ * Returns 0 when all checks hold, else a diagnostic code >= 1000.  Extension,
+ * for tests; no reference counterpart. */
+int hptt_cuda_debug_check_indexing(int dtype, uint32_t rank, const uint32_t *in_size,
+                                   const uint32_t *perm, const uint32_t *in_outer,
+                                   const uint32_t *out_outer, int max_vec_bytes,
+                                   uint64_t *checked);
+
+/* Static text for a status code. */
+const char *hptt_cuda_status_string(int status);
+
+/* Library version string. */
+const char *hptt_cuda_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* HPTT_CUDA_H_ */

@@ -1,0 +1,254 @@
+"""GPU parity: the sm_100a kernels, called through the C ABI, against the
+oracle (itself pinned to the reference) -- bit-exact for every element type,
+including the scaled cases (products and sums are rounded separately on both
+sides, no FMA), NaN matching NaN.
+
+Full-size workloads are checked through size-independent properties: exact
+samples of the index map, and permute/inverse-permute round trips.
+"""
+import numpy as np
+import pytest
+
+import oracle
+from golden.make_golden import load as load_golden
+from helpers import assert_same, footprint, gpu_run, oracle_run, random_perm, seeded
+
+pytestmark = pytest.mark.gpu
+
+torch = pytest.importorskip("torch")
+if not torch.cuda.is_available():
+    pytest.skip("no CUDA device", allow_module_level=True)
+
+import hptt_b200 as h  # noqa: E402
+
+DTYPES = ["f32", "f64", "c64", "c128"]
+SCALARS = [(1.0, 0.0), (2.3, 4.2), (-0.5, 1e-17), (0.0, 1.0)]
+
+
+@pytest.mark.parametrize("case", list(load_golden()), ids=lambda c: c["key"])
+def test_golden_fixtures(case):
+    name = case["dtype"]
+    got = gpu_run(name, case["in_size"], case["perm"], case["alpha"], case["beta"],
+                  case["a"], case["b0"])
+    assert_same(got, case["b1"], name, f"golden {case['key']}")
+
+
+def _check(name, size, perm, al, be, io=None, oo=None, cs=None, seed=0, offset=0):
+    rng = np.random.default_rng(seed)
+    n_in, n_out = footprint(size, perm, io, oo)
+    a = seeded(rng, n_in, name)
+    b0 = seeded(rng, n_out, name)
+    want = oracle_run(name, size, perm, al, be, a, b0, io, oo, complex_scalars=cs)
+    got = gpu_run(name, size, perm, al, be, a, b0, io, oo, complex_scalars=cs,
+                  device_offset_bytes=offset)
+    assert_same(got, want, name, f"{name} {size} {perm} a={al} b={be} io={io} oo={oo}")
+
+
+@pytest.mark.parametrize("seed", range(48))
+def test_random_shapes(seed):
+    rng = np.random.default_rng(1000 + seed)
+    name = DTYPES[seed % 4]
+    rank = 2 + seed % 5
+    size = [int(x) for x in np.exp(rng.uniform(0, np.log(60), rank)).astype(int) + 1]
+    while np.prod(size) > 400000:
+        size[int(np.argmax(size))] //= 2
+    perm = random_perm(rng, rank)
+    al, be = SCALARS[seed % len(SCALARS)]
+    _check(name, size, perm, al, be, seed=seed)
+
+
+@pytest.mark.parametrize("name", DTYPES)
+@pytest.mark.parametrize("perm", [[1, 0, 2], [2, 1, 0], [0, 2, 1], [1, 2, 0], [2, 0, 1]])
+def test_all_rank3_perms_ragged(name, perm):
+    _check(name, [37, 29, 23], perm, 2.3, 4.2)
+    _check(name, [37, 29, 23], perm, 1.0, 0.0)
+
+
+@pytest.mark.parametrize("name", DTYPES)
+def test_all_rank4_perms(name):
+    import itertools
+    for i, perm in enumerate(itertools.permutations(range(4))):
+        al, be = SCALARS[i % 2]
+        _check(name, [5, 7, 3, 6], list(perm), al, be, seed=i)
+
+
+@pytest.mark.parametrize("name", DTYPES)
+@pytest.mark.parametrize("lead", [1, 2, 3, 4, 8, 16, 31])
+def test_tiny_leading_extents(name, lead):
+    _check(name, [lead, 300, 7], [1, 2, 0], 2.3, 4.2)
+    _check(name, [300, lead, 7], [1, 0, 2], 1.0, 0.0)
+    _check(name, [lead, 40, 9, 5], [0, 2, 3, 1], 2.3, 4.2)  # shared stride-1
+
+
+@pytest.mark.parametrize("name", DTYPES)
+def test_outer_sizes(name):
+    _check(name, [5, 6, 7], [2, 0, 1], 2.3, 4.2, io=[8, 6, 9])
+    _check(name, [5, 6, 7], [2, 0, 1], 1.0, 0.0, oo=[9, 5, 10])
+    _check(name, [5, 6, 7], [0, 2, 1], 2.3, 4.2, io=[6, 7, 7], oo=[7, 7, 8])
+    _check(name, [64, 6, 7], [0, 1, 2], 2.3, 4.2, io=[66, 6, 7], oo=[65, 7, 7])
+
+
+@pytest.mark.parametrize("name", ["c64", "c128"])
+def test_complex_scalars(name):
+    _check(name, [8, 64, 4, 6, 2, 3], [5, 2, 0, 4, 1, 3], 1.5 - 0.5j, 0.25 + 1j, cs=True)
+    _check(name, [8, 64, 4, 6, 2, 3], [0, 3, 2, 1, 4, 5], 1.5 - 0.5j, 0.25 + 1j, cs=True)
+    _check(name, [33, 17], [1, 0], 1.5 - 0.5j, 0.0, cs=True)
+
+
+@pytest.mark.parametrize("name", DTYPES)
+def test_misaligned_pointers(name):
+    # one element off a 16-byte boundary: vector row path must fall back
+    _check(name, [64, 32, 5], [0, 2, 1], 2.3, 4.2, offset={"f32": 4, "f64": 8, "c64": 8, "c128": 16}[name])
+    _check(name, [64, 32, 5], [0, 2, 1], 1.0, 0.0, offset={"f32": 4, "f64": 8, "c64": 8, "c128": 16}[name])
+
+
+@pytest.mark.parametrize("name", ["f32", "f64"])
+def test_special_values(name):
+    rng = np.random.default_rng(5)
+    size, perm = [17, 19, 3], [2, 0, 1]
+    n = int(np.prod(size))
+    a = seeded(rng, n, name)
+    a[::7] = np.inf
+    a[1::11] = -np.inf
+    a[2::13] = np.nan
+    a[3::5] = -0.0
+    b0 = seeded(rng, n, name)
+    b0[::3] = np.nan
+    for al, be in [(1.0, 0.0), (2.3, 4.2), (-1.0, 1e-20), (0.0, 0.0)]:
+        want = oracle_run(name, size, perm, al, be, a, b0)
+        got = gpu_run(name, size, perm, al, be, a, b0)
+        assert_same(got, want, name, f"special a={al} b={be}")
+
+
+def test_identity_and_single_element():
+    _check("f32", [1000, 3, 5], [0, 1, 2], 2.3, 4.2)
+    _check("c128", [1, 1], [1, 0], 2.3, 4.2)
+    _check("f64", [1, 1, 1, 1, 1, 1], [5, 4, 3, 2, 1, 0], 2.3, 4.2)
+
+
+def test_reset_data_set_coef_and_streams():
+    name = "f32"
+    size, perm = [300, 200], [1, 0]
+    rng = np.random.default_rng(3)
+    n = 60000
+    a1, a2 = seeded(rng, n, name), seeded(rng, n, name)
+    b0 = seeded(rng, n, name)
+    da1 = torch.from_numpy(a1).cuda()
+    da2 = torch.from_numpy(a2).cuda()
+    db1 = torch.from_numpy(b0.copy()).cuda()
+    db2 = torch.from_numpy(b0.copy()).cuda()
+    plan = h.create_plan(da1, db1, size, perm, 2.3, 4.2, 0)
+    plan.exec()
+    plan.reset_data(da2, db2)
+    s = torch.cuda.Stream()
+    plan.set_stream(s)
+    plan.exec()
+    plan.sync()
+    assert_same(db1.cpu().numpy(), oracle_run(name, size, perm, 2.3, 4.2, a1, b0), name, "first")
+    assert_same(db2.cpu().numpy(), oracle_run(name, size, perm, 2.3, 4.2, a2, b0), name, "reset")
+    plan.set_coef(1.0, 0.0)
+    plan.exec_on(s)
+    s.synchronize()
+    assert_same(db2.cpu().numpy(), oracle_run(name, size, perm, 1.0, 0.0, a2, b0), name, "coef")
+    plan.set_thread_ids([0, 1])
+    plan.unset_thread_ids()
+    assert "fused rank" in plan.describe()
+
+
+def test_tuned_plan_matches():
+    _check("f64", [96, 80, 12], [2, 0, 1], 2.3, 4.2)
+    rng = np.random.default_rng(9)
+    size, perm = [96, 80, 12], [2, 0, 1]
+    n = int(np.prod(size))
+    a, b0 = seeded(rng, n, "f64"), seeded(rng, n, "f64")
+    got = gpu_run("f64", size, perm, 2.3, 4.2, a, b0, tuning_timeout=-1.0)
+    assert_same(got, oracle_run("f64", size, perm, 2.3, 4.2, a, b0), "f64", "tuned")
+
+
+# --------------------------------------------------------------------------
+# Workloads at full size
+# --------------------------------------------------------------------------
+def _sample_check(name, size, perm, al, be, a_np, b0_np, b_np, k=20000, seed=0):
+    """Exact check of k random output positions against the index formula and
+    the oracle's arithmetic (run on just those elements)."""
+    rng = np.random.default_rng(seed)
+    rank = len(size)
+    out_size = [size[p] for p in perm]
+    idx = rng.integers(0, int(np.prod(size)), k)
+    coords = np.unravel_index(idx, size, order="F")
+    ib = np.zeros(k, dtype=np.int64)
+    stride = 1
+    for kk in range(rank):
+        ib += coords[perm[kk]].astype(np.int64) * stride
+        stride *= out_size[kk]
+    a_s = np.ascontiguousarray(a_np[idx])
+    b_s = np.ascontiguousarray(b0_np[ib])
+    want = oracle_run(name, [k, 1], [0, 1], al, be, a_s, b_s,
+                      complex_scalars=isinstance(al, complex) or isinstance(be, complex))
+    assert_same(b_np[ib], want, name, f"sampled {size} {perm}")
+
+
+def test_plain_single_transpose_full_size():
+    """f32 {256,256,256}, perm {2,1,0}, alpha 2.3, beta 4.2, seed 0: bit-exact."""
+    name, size, perm = "f32", [256, 256, 256], [2, 1, 0]
+    rng = np.random.default_rng(0)
+    n = int(np.prod(size))
+    a = seeded(rng, n, name)
+    b0 = seeded(rng, n, name)
+    got = gpu_run(name, size, perm, 2.3, 4.2, a, b0)
+    want = oracle_run(name, size, perm, 2.3, 4.2, a, b0)
+    assert_same(got, want, name, "plain single transpose")
+
+
+@pytest.mark.parametrize("name,perm", [("c64", [5, 2, 0, 4, 1, 3]), ("c64", [0, 3, 2, 1, 4, 5]),
+                                       ("c128", [5, 2, 0, 4, 1, 3]), ("c128", [0, 3, 2, 1, 4, 5])])
+def test_hard_layouts_full_size(name, perm):
+    size = [8, 64, 4, 64, 16, 16] if name == "c64" else [8, 64, 4, 64, 16, 8]
+    rng = np.random.default_rng(3)
+    n = int(np.prod(size))
+    a = seeded(rng, n, name)
+    b0 = seeded(rng, n, name)
+    al, be = 1.5 - 0.5j, 0.25 + 1j
+    got = gpu_run(name, size, perm, al, be, a, b0, complex_scalars=True)
+    want = oracle_run(name, size, perm, al, be, a, b0, complex_scalars=True)
+    assert_same(got, want, name, f"hard layout {perm}")
+
+
+def _round_trip(name, size, perm):
+    """alpha=1, beta=0 is a pure permutation: perm then inverse returns A."""
+    tdt = {"f32": torch.float32, "f64": torch.float64}[name]
+    n = int(np.prod(size))
+    g = torch.Generator(device="cuda").manual_seed(7)
+    a = torch.rand(n, dtype=tdt, device="cuda", generator=g) * 2 - 1
+    b = torch.empty_like(a)
+    c = torch.empty_like(a)
+    out_size = [size[p] for p in perm]
+    inv = [0] * len(perm)
+    for k, p in enumerate(perm):
+        inv[p] = k
+    p1 = h.create_plan(a, b, size, perm, 1.0, 0.0, 0)
+    p2 = h.create_plan(b, c, out_size, inv, 1.0, 0.0, 0)
+    p1.exec()
+    p2.exec()
+    p2.sync()
+    assert torch.equal(a.view(torch.int32 if name == "f32" else torch.int64),
+                       c.view(torch.int32 if name == "f32" else torch.int64))
+    # a permutation keeps the multiset of values
+    assert torch.equal(torch.sort(a).values, torch.sort(b).values)
+    return a, b
+
+
+@pytest.mark.parametrize("seed", range(0, 48, 4))
+def test_sweep_cases_full_size(seed):
+    from hptt_b200.workloads import sweep_cases
+    case = sweep_cases()[seed]
+    name, size, perm = case["dtype"], case["in_size"], case["perm"]
+    a, b = _round_trip(name, size, perm)
+    # scaled variant, sampled exactly
+    b0 = torch.rand_like(a) * 2 - 1
+    b1 = b0.clone()
+    plan = h.create_plan(a, b1, size, perm, 2.3, 4.2, 0)
+    plan.exec()
+    plan.sync()
+    _sample_check(name, size, perm, 2.3, 4.2, a.cpu().numpy(), b0.cpu().numpy(),
+                  b1.cpu().numpy(), seed=seed)

@@ -1,0 +1,81 @@
+"""CPU replay of every launch's addressing (no GPU).
+
+hptt_cuda_debug_check_indexing plans a problem and walks every tile and
+thread with the kernels' own index helpers: all A/B/shared-memory accesses
+must stay in bounds, every inner B element must be written exactly once with
+the A element the permutation maps to it, and padding must stay untouched.
+"""
+import ctypes
+
+import numpy as np
+import pytest
+
+import hptt_b200 as h
+
+_u32p = ctypes.POINTER(ctypes.c_uint32)
+
+
+def check(dtype, size, perm, io=None, oo=None, max_vec_bytes=0):
+    lib = h.load_library()
+    f = lib.hptt_cuda_debug_check_indexing
+    f.argtypes = [ctypes.c_int, ctypes.c_uint32, _u32p, _u32p, _u32p, _u32p, ctypes.c_int,
+                  ctypes.POINTER(ctypes.c_uint64)]
+    f.restype = ctypes.c_int
+    u = lambda v: (ctypes.c_uint32 * len(v))(*v) if v is not None else None  # noqa: E731
+    n = ctypes.c_uint64(0)
+    rc = f(h.dtype_code(dtype), len(size), u(size), u(perm), u(io), u(oo), max_vec_bytes,
+           ctypes.byref(n))
+    return rc, n.value
+
+
+def _random_case(seed):
+    rng = np.random.default_rng(seed)
+    rank = int(rng.integers(2, 7))
+    dt = ["f32", "f64", "c64", "c128"][int(rng.integers(0, 4))]
+    size = [int(x) for x in np.exp(rng.uniform(0, np.log(40), rank)).astype(int) + 1]
+    while np.prod(size) > 200000:
+        size[int(np.argmax(size))] //= 2
+    perm = [int(x) for x in rng.permutation(rank)]
+    io = oo = None
+    if seed % 3 == 0:
+        io = [s + int(rng.integers(0, 3)) for s in size]
+    if seed % 5 == 0:
+        # satisfy both the reference guard and the output extents
+        oo = [max(size[p], size[perm[p]]) + int(rng.integers(0, 3)) for p in perm]
+        oo = [max(oo[k], size[perm[k]]) for k in range(rank)]
+    return dt, size, perm, io, oo
+
+
+@pytest.mark.parametrize("seed", range(600))
+def test_replay_random(seed):
+    dt, size, perm, io, oo = _random_case(seed)
+    for mv in (0, {"f32": 4, "f64": 8, "c64": 8, "c128": 16}[dt]):
+        rc, n = check(dt, size, perm, io, oo, mv)
+        if rc == 4:  # rejected by the reference's own outer-size guard
+            pytest.skip("guard")
+        assert rc == 0, (dt, size, perm, io, oo, mv, rc)
+        assert n == np.prod(size)
+
+
+SHAPES = [
+    ("f32", [256, 256, 256], [2, 1, 0]),          # plain single transpose workload
+    ("f32", [4, 100000], [1, 0]),                  # tiny input-leading extent
+    ("f32", [100000, 3], [1, 0]),                  # tiny output-leading extent
+    ("c64", [8, 64, 4, 64, 16, 2], [5, 2, 0, 4, 1, 3]),
+    ("c128", [8, 64, 4, 64, 16, 2], [0, 3, 2, 1, 4, 5]),
+    ("c64", [2, 64, 4, 16, 16, 8], [0, 3, 2, 1, 4, 5]),
+    ("f64", [4097, 513], [1, 0]),
+    ("f32", [7, 5, 3, 2, 11, 13], [5, 4, 3, 2, 1, 0]),
+    ("f64", [3, 3, 3, 3, 3, 3], [1, 0, 3, 2, 5, 4]),
+    ("f32", [1, 906, 1, 906], [2, 3, 0, 1]),
+    ("f32", [1, 1], [1, 0]),
+    ("c128", [1000, 7], [0, 1]),
+]
+
+
+@pytest.mark.parametrize("dt,size,perm", SHAPES)
+def test_replay_shapes(dt, size, perm):
+    for mv in (0, 4):
+        rc, n = check(dt, size, perm, max_vec_bytes=mv)
+        assert rc == 0, (dt, size, perm, mv, rc)
+        assert n == np.prod(size)
