@@ -6,12 +6,14 @@
 #include <cstring>
 #include <new>
 #include <string>
+#include <vector>
 
 #include "../../include/hptt_cuda.h"
 #include "autotune.h"
 #include "launch.h"
 #include "plan.h"
 #include "planner.h"
+#include "tables.h"
 
 namespace hptt_b200 {
 
@@ -48,7 +50,7 @@ void set_scalars(HpttArgs *a, const double *alpha, const double *beta,
 
 int plan_tiles(Plan *p, const TileParams &params) {
   p->params = params;
-  int st = choose_tile(p->args.p, params, &p->args.t);
+  int st = choose_tile(p->args.p, params, p->args.update, &p->args.t);
   if (st != ST_OK) return st;
   p->vec = p->args.t.kind == KIND_ROWS ? p->args.t.vec : 1;
   if (p->args.t.kind == KIND_ROWS && p->vec > 1) {
@@ -56,10 +58,32 @@ int plan_tiles(Plan *p, const TileParams &params) {
     // aligned to the planned vector
     TileParams sp = params;
     sp.max_vec_bytes = elem_bytes(p->args.p.dtype);
-    st = choose_tile(p->args.p, sp, &p->tile_scalar);
+    st = choose_tile(p->args.p, sp, p->args.update, &p->tile_scalar);
     if (st != ST_OK) return st;
   } else {
     p->tile_scalar = p->args.t;
+  }
+  // device offset tables (a few KB, read through L1 by every CTA)
+  plan_free_tables(p);
+  auto upload = [](const HpttProblem &prob, const HpttTile &t, void **dst) -> int {
+    std::vector<unsigned char> host;
+    build_tables(prob, t, &host);
+    if (cudaMalloc(dst, host.size()) != cudaSuccess) {
+      cudaGetLastError();
+      *dst = nullptr;
+      return ST_ALLOC;
+    }
+    if (cudaMemcpy(*dst, host.data(), host.size(), cudaMemcpyHostToDevice) != cudaSuccess)
+      return ST_CUDA;
+    return ST_OK;
+  };
+  st = upload(p->args.p, p->args.t, &p->dtab);
+  if (st != ST_OK) return st;
+  if (p->args.t.kind == KIND_ROWS && p->vec > 1) {
+    st = upload(p->args.p, p->tile_scalar, &p->dtab_scalar);
+    if (st != ST_OK) return st;
+  } else {
+    p->dtab_scalar = p->dtab;
   }
   // grid: resident CTAs on every SM, capped by the tile count
   auto size_grid = [&](const HpttTile &t, int vec, int *grid) -> int {
@@ -92,13 +116,22 @@ int plan_enqueue(Plan *p, cudaStream_t stream) {
   const int vec = plan_vec_for_ptrs(p);
   cudaError_t e;
   if (vec == p->vec) {
+    p->args.tables = p->dtab;
     e = launch_single(p->args, vec, p->grid, stream);
   } else {
     HpttArgs a = p->args;
     a.t = p->tile_scalar;
+    a.tables = p->dtab_scalar;
     e = launch_single(a, 1, p->grid_scalar, stream);
   }
   return e == cudaSuccess ? ST_OK : ST_CUDA;
+}
+
+void plan_free_tables(Plan *p) {
+  if (p->dtab_scalar && p->dtab_scalar != p->dtab) cudaFree(p->dtab_scalar);
+  if (p->dtab) cudaFree(p->dtab);
+  p->dtab = nullptr;
+  p->dtab_scalar = nullptr;
 }
 
 }  // namespace hptt_b200
@@ -155,6 +188,7 @@ int hptt_cuda_plan_create(int dtype, uint32_t rank, const uint32_t *in_size,
   st = plan_tiles(p, params);
   if (st != ST_OK && have) st = plan_tiles(p, TileParams());
   if (st != ST_OK) {
+    plan_free_tables(p);
     delete p;
     return st;
   }
@@ -246,6 +280,7 @@ int hptt_cuda_plan_destroy(hptt_cuda_plan_t plan) {
   Plan *p = reinterpret_cast<Plan *>(plan);
   if (!plan_valid(p)) return HPTT_ERR_HANDLE;
   p->magic = 0;
+  plan_free_tables(p);
   delete p;
   return HPTT_OK;
 }
@@ -262,7 +297,7 @@ int hptt_cuda_plan_inspect(int dtype, uint32_t rank, const uint32_t *in_size,
   st = fuse(dtype, static_cast<int>(rank), in_size, perm, in_outer, out_outer, &p);
   if (st != ST_OK) return st;
   HpttTile t;
-  st = choose_tile(p, TileParams(), &t);
+  st = choose_tile(p, TileParams(), 0, &t);
   if (st != ST_OK) return st;
   const std::string s = describe(p, t);
   if (buf && len) {

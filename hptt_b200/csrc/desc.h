@@ -65,13 +65,51 @@ struct HpttTile {
   int32_t wc;                 // chunked W dim (KIND_ROWS), -1 when none
   // grid: tile index -> origin.  gd = input dim, gcnt = number of positions,
   // gstep = tile extent along that dim (1 for dims outside the tile).
+  int32_t px, py;             // extent products of the full X (Y) dims before
+                              // the chunked last one: x = rest + px * c_last
   int32_t ng;
   int32_t gd[HPTT_MAX_RANK];
   uint32_t gcnt[HPTT_MAX_RANK];
+  uint32_t gmul[HPTT_MAX_RANK];  // fast division by gcnt: q = umulhi(n, gmul) >> gshr
+  int32_t gshr[HPTT_MAX_RANK];   // (gmul = 0 encodes gcnt == 1)
   int32_t gstep[HPTT_MAX_RANK];
   uint32_t num_tiles;
   int32_t big_offsets;        // 1 when in-tile offsets need 64 bits
   int32_t smem_bytes;         // dynamic shared memory for one CTA
+  // Byte offsets inside the plan's device table buffer (HpttArgs::tables).
+  // KIND_TILE:
+  //   [0]         TY x HpttTabEnt: row slot q -> {A offset of the row, its
+  //               coordinate along the chunked Y dim}; slots enumerate the Y
+  //               dims in INPUT order, so consecutive slots are adjacent in A
+  //   [tab2_off]  TX x HpttTabEnt: column slot q -> {B offset of the column,
+  //               its coordinate along the chunked X dim}; slots enumerate the
+  //               X dims in OUTPUT order, so consecutive slots are adjacent in B
+  //   [thr_off]   nt x HpttThr per-thread constants
+  // KIND_ROWS: A row offsets (TY x OffT) at 0, B row offsets at tab2_off.
+  int32_t tab2_off, thr_off, table_bytes;
+};
+
+// One slot of a KIND_TILE offset table (OffT = uint32_t or int64_t).
+template <typename OffT>
+struct alignas(sizeof(OffT) * 2) HpttTabEnt {
+  OffT off;
+  int32_t c;  // coordinate along the chunked dim (0 when none is chunked)
+};
+
+// Per-thread constants of the tile transpose, precomputed on the host.
+// Load phase: the thread owns element e (= w + W*x) of every row slot
+// q0 + j*R1; store phase: element e2 (= w + W*y) of every column slot
+// qs0 + j*R2.
+struct alignas(16) HpttThr {
+  int64_t inE;     // A offset of element e
+  int64_t outE2;   // B offset of element e2
+  int32_t q0, qs0; // first row slot (load), first column slot (store)
+  int32_t sme;     // shared-memory column of element e: qcol(x) * W + w
+  int32_t sme2;    // shared-memory row start of element e2: qrow(y) * LD + w
+  int32_t cxe;     // coordinate of e along the chunked X dim (0 if none)
+  int32_t cye2;    // coordinate of e2 along the chunked Y dim (0 if none)
+  int32_t active;  // bit 0: loads, bit 1: stores
+  int32_t pad;
 };
 
 // Per-thread iterations of one phase, sized so every thread keeps about 64
@@ -85,8 +123,9 @@ HPTT_HD constexpr int hptt_jmax_tile(int elem_bytes) {
   return elem_bytes >= 16 ? 4 : (elem_bytes >= 8 ? 8 : 16);
 }
 HPTT_HD constexpr int hptt_jmax_rows(int access_bytes) {
-  return access_bytes >= 16 ? 8 : 16;
+  return access_bytes >= 16 ? 4 : (access_bytes >= 8 ? 8 : 16);
 }
+
 
 // Everything one launch (or one batch entry) needs.
 struct HpttArgs {
@@ -94,6 +133,7 @@ struct HpttArgs {
   HpttTile t;
   const void *A;
   void *B;
+  const void *tables;  // device buffer laid out as HpttTile::tab2_off/thr_off say
   double alpha[2];
   double beta[2];
   int32_t mode;

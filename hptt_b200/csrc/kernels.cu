@@ -12,70 +12,27 @@ namespace {
 
 constexpr int kNT = 256;
 
-// Copy the launch arguments into shared memory with compile-time-indexed
-// word moves, so the kernels index dims dynamically from shared memory
-// rather than from the parameter space.
-__device__ __forceinline__ void stage_args(const HpttArgs &src, HpttArgs *dst) {
-  static_assert(sizeof(HpttArgs) % 8 == 0, "HpttArgs must be 8-byte sized");
-  constexpr int kWords = sizeof(HpttArgs) / 8;
-  const uint64_t *s = reinterpret_cast<const uint64_t *>(&src);
-  uint64_t *d = reinterpret_cast<uint64_t *>(dst);
-#pragma unroll
-  for (int i = 0; i < kWords; i += 32) {
-    const int w = i + static_cast<int>(threadIdx.x % 32);
-    if (threadIdx.x < 32 && w < kWords) d[w] = s[w];
-  }
-}
-
+// One CTA per tile.  The arguments live in the parameter space
+// (__grid_constant__) and are read through a const reference.
 template <typename E, int MODE, bool UPD, typename OffT>
-__global__ void __launch_bounds__(kNT, 3) k_tile(const __grid_constant__ HpttArgs args) {
+__global__ void __launch_bounds__(kNT) k_tile(const __grid_constant__ HpttArgs args) {
   extern __shared__ __align__(16) unsigned char smem[];
-  __shared__ HpttArgs sa;
-  stage_args(args, &sa);
-  __syncthreads();
-  const HpttProblem &P = sa.p;
-  const HpttTile &T = sa.t;
-  E *sdata = reinterpret_cast<E *>(smem);
-  const int data_bytes = align16(T.TY * T.LD * static_cast<int>(sizeof(E)));
-  OffT *tInY = reinterpret_cast<OffT *>(smem + data_bytes);
-  OffT *tOutX = tInY + T.TY;
-  int *tCy = reinterpret_cast<int *>(tOutX + T.TX);
-  int *tCx = tCy + T.TY;
-  tile_tables<OffT>(P, T, tInY, tCy, tOutX, tCx, threadIdx.x, blockDim.x);
-  const TileThread<OffT> s = tile_thread<OffT>(P, T, threadIdx.x);
-  const Scal sc{sa.alpha[0], sa.alpha[1], sa.beta[0], sa.beta[1]};
+  const Scal sc{args.alpha[0], args.alpha[1], args.beta[0], args.beta[1]};
   const Op<E, MODE, UPD> op(sc);
-  const E *A = static_cast<const E *>(sa.A);
-  E *B = static_cast<E *>(sa.B);
-  __syncthreads();
-  for (uint32_t tile = blockIdx.x; tile < T.num_tiles; tile += gridDim.x) {
-    const TileOrigin o = tile_origin(P, T, tile);
-    tile_body<E, MODE, UPD, OffT>(T, A, B, op, s, o, sdata, tInY, tCy, tOutX, tCx);
-  }
+  tile_one<E, MODE, UPD, OffT>(args.p, args.t, static_cast<const E *>(args.A),
+                               static_cast<E *>(args.B),
+                               static_cast<const unsigned char *>(args.tables), op,
+                               reinterpret_cast<E *>(smem), blockIdx.x);
 }
 
 template <typename E, int MODE, bool UPD, typename OffT, int VEC>
-__global__ void __launch_bounds__(kNT, 2) k_rows(const __grid_constant__ HpttArgs args) {
-  extern __shared__ __align__(16) unsigned char smem[];
-  __shared__ HpttArgs sa;
-  stage_args(args, &sa);
-  __syncthreads();
-  const HpttProblem &P = sa.p;
-  const HpttTile &T = sa.t;
-  OffT *tInY = reinterpret_cast<OffT *>(smem);
-  OffT *tOutY = tInY + T.TY;
-  int *tCy = reinterpret_cast<int *>(tOutY + T.TY);
-  rows_tables<OffT>(P, T, tInY, tOutY, tCy, threadIdx.x, blockDim.x);
-  const RowThread<OffT> s = rows_thread<OffT>(T, threadIdx.x);
-  const Scal sc{sa.alpha[0], sa.alpha[1], sa.beta[0], sa.beta[1]};
+__global__ void __launch_bounds__(kNT) k_rows(const __grid_constant__ HpttArgs args) {
+  const Scal sc{args.alpha[0], args.alpha[1], args.beta[0], args.beta[1]};
   const Op<E, MODE, UPD> op(sc);
-  const E *A = static_cast<const E *>(sa.A);
-  E *B = static_cast<E *>(sa.B);
-  __syncthreads();
-  for (uint32_t tile = blockIdx.x; tile < T.num_tiles; tile += gridDim.x) {
-    const TileOrigin o = tile_origin(P, T, tile);
-    rows_body<E, MODE, UPD, OffT, VEC>(P, T, A, B, op, s, o, tInY, tOutY, tCy);
-  }
+  rows_one<E, MODE, UPD, OffT, VEC>(args.p, args.t, static_cast<const E *>(args.A),
+                                    static_cast<E *>(args.B),
+                                    static_cast<const unsigned char *>(args.tables), op,
+                                    blockIdx.x);
 }
 
 // ---------------------------------------------------------------------------
@@ -137,19 +94,28 @@ const void *kernel_for(const HpttArgs &a, int vec) {
 int kernel_threads() { return kNT; }
 
 cudaError_t launch_single(const HpttArgs &a, int vec, int grid, cudaStream_t stream) {
+  (void)grid;
   const void *fn = kernel_for(a, vec);
   if (!fn) return cudaErrorInvalidValue;
   if (a.t.num_tiles == 0) return cudaSuccess;
   void *params[] = {const_cast<HpttArgs *>(&a)};
-  return cudaLaunchKernel(fn, dim3(grid), dim3(a.t.nt), params,
+  return cudaLaunchKernel(fn, dim3(a.t.num_tiles), dim3(a.t.nt), params,
                           static_cast<size_t>(a.t.smem_bytes), stream);
 }
 
 cudaError_t occupancy(const HpttArgs &a, int vec, int *ctas_per_sm) {
   const void *fn = kernel_for(a, vec);
   if (!fn) return cudaErrorInvalidValue;
-  cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       a.t.smem_bytes > 48 * 1024 ? a.t.smem_bytes : 48 * 1024);
+  // One kernel serves many plans: always allow the device's opt-in maximum,
+  // so a later plan with a smaller tile cannot lower the limit under an
+  // earlier one.
+  int dev = 0, optin = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+  if (e != cudaSuccess) return e;
+  if (a.t.smem_bytes > optin) return cudaErrorInvalidValue;
+  e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, optin);
   if (e != cudaSuccess) return e;
   return cudaOccupancyMaxActiveBlocksPerMultiprocessor(ctas_per_sm, fn, a.t.nt,
                                                        static_cast<size_t>(a.t.smem_bytes));

@@ -25,7 +25,12 @@ struct Plan {
   uint64_t elements = 0;    // N = prod(in_size)
   TileParams params;        // chosen by heuristic or tuner
   bool tuned = false;
+  void *dtab = nullptr;         // device offset tables for args.t
+  void *dtab_scalar = nullptr;  // ... and for tile_scalar (may alias dtab)
 };
+
+// Release the plan's device tables.
+void plan_free_tables(Plan *p);
 
 // Fill scalars/mode/update from alpha, beta.
 void set_scalars(HpttArgs *a, const double *alpha, const double *beta,

@@ -171,6 +171,101 @@ int fuse(int dtype, int rank, const uint32_t *in_size, const uint32_t *perm,
 
 namespace {
 
+// Enumerate the digits of a tile-local mixed-radix index in a chosen order.
+//   dims/ext: the side's dims and tile extents in the side's own order (the
+//   index's radix order, first fastest); order: permutation of 0..nd-1 giving
+//   the enumeration order (first fastest).  For every slot q, returns the
+//   index in the side's own order, its offset with `stride`, and its
+//   coordinate along `chunk_dim` (0 when that dim is not on this side).
+void enumerate(int nd, const int32_t *dims, const int32_t *ext, const int *order,
+               const int64_t *stride, int chunk_dim, std::vector<int> *idx,
+               std::vector<int64_t> *off, std::vector<int> *chunk) {
+  int64_t place[HPTT_MAX_RANK];
+  int64_t total = 1;
+  for (int i = 0; i < nd; ++i) {
+    place[i] = total;
+    total *= ext[i];
+  }
+  idx->assign(static_cast<size_t>(total), 0);
+  off->assign(static_cast<size_t>(total), 0);
+  chunk->assign(static_cast<size_t>(total), 0);
+  for (int64_t q = 0; q < total; ++q) {
+    int64_t rem = q, id = 0, o = 0;
+    int cc = 0;
+    for (int k = 0; k < nd; ++k) {
+      const int i = order[k];
+      const int64_t c = rem % ext[i];
+      rem /= ext[i];
+      id += c * place[i];
+      o += c * stride[dims[i]];
+      if (dims[i] == chunk_dim) cc = static_cast<int>(c);
+    }
+    (*idx)[q] = static_cast<int>(id);
+    (*off)[q] = o;
+    (*chunk)[q] = cc;
+  }
+}
+
+// Coordinate of side-order index `idx` along `chunk_dim`, and its offset.
+int64_t side_offset(int idx, int nd, const int32_t *dims, const int32_t *ext,
+                    const int64_t *stride, int chunk_dim, int *chunk) {
+  int64_t o = 0;
+  *chunk = 0;
+  for (int i = 0; i < nd; ++i) {
+    const int c = idx % ext[i];
+    idx /= ext[i];
+    o += static_cast<int64_t>(c) * stride[dims[i]];
+    if (dims[i] == chunk_dim) *chunk = c;
+  }
+  return o;
+}
+
+}  // namespace
+
+void tile_maps(const HpttProblem &p, const HpttTile &t, TileMaps *m) {
+  int order[HPTT_MAX_RANK];
+  std::vector<int> slot_to_y, slot_to_x;
+  // rows: Y dims in input order
+  for (int i = 0; i < t.ny; ++i) order[i] = i;
+  std::sort(order, order + t.ny, [&](int a, int b) { return t.yd[a] < t.yd[b]; });
+  enumerate(t.ny, t.yd, t.yt, order, p.sA, t.yc, &slot_to_y, &m->offA, &m->cy);
+  // columns: X dims in output order
+  int pos[HPTT_MAX_RANK];
+  for (int k = 0; k < p.rank; ++k) pos[p.perm[k]] = k;
+  for (int i = 0; i < t.nx; ++i) order[i] = i;
+  std::sort(order, order + t.nx, [&](int a, int b) { return pos[t.xd[a]] < pos[t.xd[b]]; });
+  enumerate(t.nx, t.xd, t.xt, order, p.sB, t.xc, &slot_to_x, &m->offB, &m->cx);
+  m->qrow.assign(slot_to_y.size(), 0);
+  for (size_t q = 0; q < slot_to_y.size(); ++q) m->qrow[slot_to_y[q]] = static_cast<int>(q);
+  m->qcol.assign(slot_to_x.size(), 0);
+  for (size_t q = 0; q < slot_to_x.size(); ++q) m->qcol[slot_to_x[q]] = static_cast<int>(q);
+}
+
+HpttThr tile_thread_consts(const HpttProblem &p, const HpttTile &t, const TileMaps &m,
+                           int tid) {
+  HpttThr h;
+  std::memset(&h, 0, sizeof(h));
+  const bool ld = tid < t.R1 * t.RW, st = tid < t.R2 * t.WTY;
+  h.active = (ld ? 1 : 0) | (st ? 2 : 0);
+  {
+    const int e = tid % t.RW, w = e % t.W, x = e / t.W;
+    h.q0 = tid / t.RW;
+    h.inE = side_offset(x, t.nx, t.xd, t.xt, p.sA, t.xc, &h.cxe) +
+            static_cast<int64_t>(w) * p.sA[0];
+    h.sme = m.qcol[x] * t.W + w;
+  }
+  {
+    const int e2 = tid % t.WTY, w = e2 % t.W, y = e2 / t.W;
+    h.qs0 = tid / t.WTY;
+    h.outE2 = side_offset(y, t.ny, t.yd, t.yt, p.sB, t.yc, &h.cye2) +
+              static_cast<int64_t>(w) * p.sB[0];
+    h.sme2 = m.qrow[y] * t.LD + w;
+  }
+  return h;
+}
+
+namespace {
+
 int64_t cdiv(int64_t a, int64_t b) { return (a + b - 1) / b; }
 
 // Shared-memory wavefronts for one warp whose lanes access byte addresses
@@ -194,29 +289,32 @@ int excess_wavefronts(const int64_t *addr, int lanes, int bytes) {
   return static_cast<int>(worst) - std::max(ideal, 1);
 }
 
-int bank_cost(const HpttTile &t, int ld, int sz) {
+// Shared-memory wavefronts beyond the ideal for the first warps of both
+// phases with row pitch `ld` (same addressing as tile_one).
+int bank_cost(const HpttTile &t, int ld, int sz, const TileMaps &m) {
   int cost = 0;
   int64_t addr[32];
   const int warps = std::min(t.nt / 32, 4);
   for (int w = 0; w < warps; ++w) {
-    // load phase: thread -> (e, y0), element at y*LD + e
+    // load phase: thread (e, q0) writes row slot q0 at column qcol(x)*W + w
     for (int l = 0; l < 32; ++l) {
       const int tid = w * 32 + l;
       if (tid < t.R1 * t.RW) {
-        const int e = tid % t.RW, y = tid / t.RW;
-        addr[l] = (y < t.TY) ? static_cast<int64_t>(y * ld + e) * sz : -1;
+        const int e = tid % t.RW, q = tid / t.RW;
+        const int col = m.qcol[e / t.W] * t.W + e % t.W;
+        addr[l] = (q < t.TY) ? static_cast<int64_t>(q * ld + col) * sz : -1;
       } else {
         addr[l] = -1;
       }
     }
     cost += excess_wavefronts(addr, 32, sz);
-    // store phase: thread -> (e2, x0); e2 = w + W*y; element at y*LD + w + W*x
+    // store phase: thread (e2, qs0) reads row qrow(y) at column qs0*W + w
     for (int l = 0; l < 32; ++l) {
       const int tid = w * 32 + l;
       if (tid < t.R2 * t.WTY) {
-        const int e2 = tid % t.WTY, x = tid / t.WTY;
+        const int e2 = tid % t.WTY, q = tid / t.WTY;
         const int ww = e2 % t.W, y = e2 / t.W;
-        addr[l] = (x < t.TX) ? static_cast<int64_t>(y * ld + ww + t.W * x) * sz : -1;
+        addr[l] = (q < t.TX) ? static_cast<int64_t>(m.qrow[y] * ld + ww + t.W * q) * sz : -1;
       } else {
         addr[l] = -1;
       }
@@ -244,7 +342,7 @@ bool shape_ok(const TileParams &tp, int64_t W, const Side &X, const Side &Y,
   if (RW > tp.nt || WTY > tp.nt) return false;
   const int64_t R1 = tp.nt / RW, R2 = tp.nt / WTY;
   if (cdiv(TY, R1) > kJMax || cdiv(TX, R2) > kJMax) return false;
-  if ((RW + 31) * TY * sz > tp.smem_bytes + 32 * TY * sz) return false;
+  if (RW * TY * sz > tp.smem_bytes) return false;
   return true;
 }
 
@@ -270,6 +368,22 @@ void finish_grid(const HpttProblem &p, HpttTile *t, const int64_t *tile_ext,
   for (int d = 0; d < p.rank; ++d)
     if (!used[d]) add(d);
   t->num_tiles = tiles > 0x7fffffffULL ? 0 : static_cast<uint32_t>(tiles);
+  // Division by a run-time constant as multiply-high and shift, exact for
+  // dividends below 2^31 (tile indices are): with l = ceil(log2 d) and
+  // p = 31 + l, m = ceil(2^p / d) and n / d = (n * m) >> p.
+  for (int g = 0; g < t->ng; ++g) {
+    const uint32_t d = t->gcnt[g];
+    if (d <= 1) {
+      t->gmul[g] = 0;
+      t->gshr[g] = 0;
+      continue;
+    }
+    int l = 0;
+    while ((1ull << l) < d) ++l;
+    const int pw = 31 + l;
+    t->gmul[g] = static_cast<uint32_t>(((1ull << pw) + d - 1) / d);
+    t->gshr[g] = pw - 32;
+  }
 }
 
 int choose_rows(const HpttProblem &p, const TileParams &tp, HpttTile *t) {
@@ -320,6 +434,9 @@ int choose_rows(const HpttProblem &p, const TileParams &tp, HpttTile *t) {
   }
   t->TY = static_cast<int32_t>(TY);
   t->TX = 1;
+  t->px = 1;
+  t->py = 1;
+  for (int i = 0; i + 1 < t->ny; ++i) t->py *= t->yt[i];
   t->J1 = static_cast<int32_t>(cdiv(TY, t->R1));
   t->WTY = t->W;
   t->LD = 0;
@@ -332,13 +449,16 @@ int choose_rows(const HpttProblem &p, const TileParams &tp, HpttTile *t) {
   }
   t->big_offsets = (maxA >= 0x7fffffffLL || maxB >= 0x7fffffffLL);
   const int off = t->big_offsets ? 8 : 4;
-  t->smem_bytes = static_cast<int32_t>(TY * (2 * off + 4));
+  t->smem_bytes = 0;
+  t->tab2_off = (t->TY * off + 15) & ~15;
+  t->thr_off = t->tab2_off + ((t->TY * off + 15) & ~15);
+  t->table_bytes = t->thr_off;
   return t->num_tiles ? ST_OK : ST_TOO_LARGE;
 }
 
 }  // namespace
 
-int choose_tile(const HpttProblem &p, const TileParams &tp, HpttTile *t) {
+int choose_tile(const HpttProblem &p, const TileParams &tp, int update, HpttTile *t) {
   const int sz = elem_bytes(p.dtype);
   const int r = p.rank;
   const bool common = p.perm[0] == 0;
@@ -456,6 +576,22 @@ int choose_tile(const HpttProblem &p, const TileParams &tp, HpttTile *t) {
     }
     if (!grown) break;
   }
+  // Chunked last dims: take the whole extent when it is only a little larger
+  // than the chunk, else split it into equal chunks, so edge tiles are not
+  // mostly empty (72 = 64 + 8 becomes 2 x 36).
+  for (Side *S : {&X, &Y}) {
+    if (S->d.empty()) continue;
+    const int64_t n = p.n[S->d.back()];
+    int64_t &tt = S->t.back();
+    if (tt >= n) continue;
+    const int64_t old = tt;
+    if (2 * n <= 3 * tt) {
+      tt = n;
+      if (shape_ok(tp, W, X, Y, sz)) continue;
+      tt = old;
+    }
+    tt = cdiv(n, cdiv(n, old));
+  }
   if (!shape_ok(tp, W, X, Y, sz)) return ST_TOO_LARGE;
 
   t->W = static_cast<int32_t>(W);
@@ -477,6 +613,10 @@ int choose_tile(const HpttProblem &p, const TileParams &tp, HpttTile *t) {
   if (t->nx && X.t.back() < p.n[X.d.back()]) t->xc = X.d.back();
   if (t->ny && Y.t.back() < p.n[Y.d.back()]) t->yc = Y.d.back();
   t->TX = static_cast<int32_t>(X.prod());
+  t->px = 1;
+  t->py = 1;
+  for (int i = 0; i + 1 < t->nx; ++i) t->px *= t->xt[i];
+  for (int i = 0; i + 1 < t->ny; ++i) t->py *= t->yt[i];
   t->TY = static_cast<int32_t>(Y.prod());
   t->RW = static_cast<int32_t>(W * t->TX);
   t->WTY = static_cast<int32_t>(W * t->TY);
@@ -485,10 +625,12 @@ int choose_tile(const HpttProblem &p, const TileParams &tp, HpttTile *t) {
   t->R2 = t->nt / t->WTY;
   t->J2 = static_cast<int32_t>(cdiv(t->TX, t->R2));
   // row pitch with the fewest shared-memory bank conflicts
+  TileMaps maps;
+  tile_maps(p, *t, &maps);
   int best_ld = t->RW, best_cost = 1 << 30;
   const int span = std::max(1, 128 / sz);
   for (int ld = t->RW; ld < t->RW + span; ++ld) {
-    const int c = bank_cost(*t, ld, sz);
+    const int c = bank_cost(*t, ld, sz, maps);
     if (c < best_cost) {
       best_cost = c;
       best_ld = ld;
@@ -513,8 +655,13 @@ int choose_tile(const HpttProblem &p, const TileParams &tp, HpttTile *t) {
   }
   t->big_offsets = (maxA >= 0x7fffffffLL || maxB >= 0x7fffffffLL);
   const int off = t->big_offsets ? 8 : 4;
-  const int64_t data = (static_cast<int64_t>(t->TY) * t->LD * sz + 15) / 16 * 16;
-  t->smem_bytes = static_cast<int32_t>(data + (t->TY + t->TX) * (off + 4));
+  (void)update;
+  t->smem_bytes = (t->TY * t->LD * sz + 15) & ~15;
+  auto a16 = [](int x) { return (x + 15) & ~15; };
+  const int ent = 2 * off;  // sizeof(HpttTabEnt<OffT>)
+  t->tab2_off = a16(t->TY * ent);
+  t->thr_off = t->tab2_off + a16(t->TX * ent);
+  t->table_bytes = t->thr_off + t->nt * static_cast<int>(sizeof(HpttThr));
   return t->num_tiles ? ST_OK : ST_TOO_LARGE;
 }
 

@@ -3,6 +3,7 @@
 
 #include <stdint.h>
 #include <string>
+#include <vector>
 
 #include "desc.h"
 
@@ -52,9 +53,26 @@ int fuse(int dtype, int rank, const uint32_t *in_size, const uint32_t *perm,
          HpttProblem *out);
 
 // Choose tile and grid.  Returns ST_OK or ST_TOO_LARGE.
-int choose_tile(const HpttProblem &p, const TileParams &tp, HpttTile *t);
+// `update` != 0 when B is read (its tile is staged in shared memory too).
+int choose_tile(const HpttProblem &p, const TileParams &tp, int update, HpttTile *t);
 
 int elem_bytes(int dtype);
+
+// Host-side index maps of a KIND_TILE tile.  Row slots enumerate the Y dims
+// in INPUT order (consecutive slots are adjacent in A); column slots
+// enumerate the X dims in OUTPUT order (consecutive slots are adjacent in B).
+struct TileMaps {
+  std::vector<int> qrow;      // row index y (Y order) -> row slot
+  std::vector<int> qcol;      // column index x (X order) -> column slot
+  std::vector<int64_t> offA;  // row slot -> A offset
+  std::vector<int> cy;        // row slot -> coordinate along the chunked Y dim
+  std::vector<int64_t> offB;  // column slot -> B offset
+  std::vector<int> cx;        // column slot -> coordinate along the chunked X dim
+};
+void tile_maps(const HpttProblem &p, const HpttTile &t, TileMaps *m);
+
+// Per-thread constants of thread `tid` (uses t.LD).
+HpttThr tile_thread_consts(const HpttProblem &p, const HpttTile &t, const TileMaps &m, int tid);
 
 // Human-readable plan summary (print_plan()).
 std::string describe(const HpttProblem &p, const HpttTile &t);

@@ -1,8 +1,8 @@
 // Host emulation of the kernels' addressing, for CPU tests.
 //
-// Runs the planner, then replays every tile and every thread of the launch
-// with the same index helpers the kernels use (kernels.cuh, compiled for the
-// host here) and checks, without a GPU:
+// Runs the planner, builds the same offset tables a plan uploads, then
+// replays every CTA (one per tile) and every thread of the launch exactly as
+// tile_one / rows_one in kernels.cuh index memory, and checks, without a GPU:
 //   - every A read and every B read/write is inside the caller's buffers,
 //   - every shared-memory access is inside the tile buffer and reads a slot
 //     the load phase of the same tile wrote,
@@ -16,6 +16,7 @@
 #include "../../include/hptt_cuda.h"
 #include "kernels.cuh"
 #include "planner.h"
+#include "tables.h"
 
 namespace hptt_b200 {
 namespace {
@@ -26,7 +27,7 @@ struct Layout {
   int rank;
   std::vector<int64_t> in_size, in_outer, out_outer, perm;
   int64_t nA = 1, nB = 1;
-  std::vector<int64_t> sa, sbo;  // input strides; output strides per output dim
+  std::vector<int64_t> sbo;  // output strides per output dim
 };
 
 // A index -> expected B index, or -1 if the A index is padding.
@@ -55,56 +56,60 @@ bool b_is_inner(const Layout &L, int64_t ib) {
 
 template <typename OffT>
 int replay_tile(const HpttProblem &P, const HpttTile &T, const Layout &L,
-                std::vector<uint8_t> &writes, uint64_t *checked) {
-  std::vector<OffT> tInY(T.TY), tOutX(T.TX);
-  std::vector<int> tCy(T.TY), tCx(T.TX);
-  tile_tables<OffT>(P, T, tInY.data(), tCy.data(), tOutX.data(), tCx.data(), 0, 1);
-  std::vector<TileThread<OffT>> th(T.nt);
-  for (int t = 0; t < T.nt; ++t) th[t] = tile_thread<OffT>(P, T, t);
+                const std::vector<unsigned char> &tab, std::vector<uint8_t> &writes,
+                uint64_t *checked) {
   const int esz = elem_bytes(P.dtype);
   const int J = hptt_jmax_tile(esz);
   if (T.J1 > J || T.J2 > J) return 101;
+  if (T.smem_bytes < T.TY * T.LD * esz) return 102;
+  using Ent = HpttTabEnt<OffT>;
+  if (T.tab2_off < T.TY * static_cast<int>(sizeof(Ent))) return 103;
+  if (T.thr_off < T.tab2_off + T.TX * static_cast<int>(sizeof(Ent))) return 104;
+  if (T.table_bytes < T.thr_off + T.nt * static_cast<int>(sizeof(HpttThr))) return 105;
+  if (T.thr_off % 16 || T.tab2_off % 16) return 106;
+  const Ent *tabY = reinterpret_cast<const Ent *>(tab.data());
+  const Ent *tabX = reinterpret_cast<const Ent *>(tab.data() + T.tab2_off);
+  const HpttThr *thr = reinterpret_cast<const HpttThr *>(tab.data() + T.thr_off);
   const int64_t smem_elems = static_cast<int64_t>(T.TY) * T.LD;
-  if (align16(static_cast<int>(smem_elems * esz)) + (T.TY + T.TX) * (static_cast<int>(sizeof(OffT)) + 4) >
-      T.smem_bytes)
-    return 102;
   std::vector<int64_t> slot(smem_elems);
   for (uint32_t tile = 0; tile < T.num_tiles; ++tile) {
     const TileOrigin o = tile_origin(P, T, tile);
-    std::fill(slot.begin(), slot.end(), -2);
+    std::fill(slot.begin(), slot.end(), -1);
+    // load phase: every in-range slot is written (garbage when invalid)
     for (int t = 0; t < T.nt; ++t) {
-      const TileThread<OffT> &s = th[t];
-      if (!s.ld_active) continue;
+      const HpttThr &th = thr[t];
+      if (!((th.active & 1) && th.cxe < o.remX)) continue;
       for (int j = 0; j < J; ++j) {
-        const int y = s.y0 + j * T.R1;
-        if (!(j < T.J1 && y < T.TY)) continue;
-        const int64_t si = static_cast<int64_t>(y) * T.LD + s.sme;
-        if (si < 0 || si >= smem_elems) return 103;
-        if (o.interior || (s.cxe < o.remX && tCy[y] < o.remY)) {
-          const int64_t ia = o.bA + static_cast<int64_t>(s.inE) + static_cast<int64_t>(tInY[y]);
-          if (ia < 0 || ia >= L.nA) return 104;
-          if (slot[si] != -2) return 105;  // two writers of one slot
+        const int q = th.q0 + j * T.R1;
+        if (!(j < T.J1 && q < T.TY)) continue;
+        const int64_t si = static_cast<int64_t>(q) * T.LD + th.sme;
+        if (si < 0 || si >= smem_elems) return 108;
+        if (slot[si] >= 0 || slot[si] == -3) return 110;  // two writers of one slot
+        if (tabY[q].c < o.remY) {
+          const int64_t ia = o.bA + th.inE + static_cast<int64_t>(tabY[q].off);
+          if (ia < 0 || ia >= L.nA) return 109;
           slot[si] = ia;
         } else {
-          if (slot[si] == -2) slot[si] = -1;  // written with an unused value
+          slot[si] = -3;  // written, value unused
         }
       }
     }
+    // store phase (and the B reads of the load phase, same addresses)
     for (int t = 0; t < T.nt; ++t) {
-      const TileThread<OffT> &s = th[t];
-      if (!s.st_active) continue;
+      const HpttThr &th = thr[t];
+      if (!((th.active & 2) && th.cye2 < o.remY)) continue;
       for (int j = 0; j < J; ++j) {
-        const int x = s.x0 + j * T.R2;
-        if (!(j < T.J2 && x < T.TX)) continue;
-        if (!(o.interior || (s.cye2 < o.remY && tCx[x] < o.remX))) continue;
-        const int64_t si = static_cast<int64_t>(s.sme2) + static_cast<int64_t>(x) * T.W;
-        if (si < 0 || si >= smem_elems) return 106;
+        const int q = th.qs0 + j * T.R2;
+        if (!(j < T.J2 && q < T.TX)) continue;
+        if (!(tabX[q].c < o.remX)) continue;
+        const int64_t si = static_cast<int64_t>(th.sme2) + static_cast<int64_t>(q) * T.W;
+        if (si < 0 || si >= smem_elems) return 112;
         const int64_t ia = slot[si];
-        if (ia < 0) return 107;  // reads a slot no valid load wrote
-        const int64_t ib = o.bB + static_cast<int64_t>(s.outE2) + static_cast<int64_t>(tOutX[x]);
-        if (ib < 0 || ib >= L.nB) return 108;
-        if (map_a_to_b(L, ia) != ib) return 109;
-        if (writes[ib] != 0) return 110;
+        if (ia < 0) return 113;  // reads a slot no valid load wrote
+        const int64_t ib = o.bB + th.outE2 + static_cast<int64_t>(tabX[q].off);
+        if (ib < 0 || ib >= L.nB) return 114;
+        if (map_a_to_b(L, ia) != ib) return 115;
+        if (writes[ib] != 0) return 116;
         writes[ib] = 1;
         ++*checked;
       }
@@ -114,35 +119,39 @@ int replay_tile(const HpttProblem &P, const HpttTile &T, const Layout &L,
 }
 
 template <typename OffT>
-int replay_rows(const HpttProblem &P, const HpttTile &T, const Layout &L, int vec,
-                std::vector<uint8_t> &writes, uint64_t *checked) {
-  std::vector<OffT> tInY(T.TY), tOutY(T.TY);
-  std::vector<int> tCy(T.TY);
-  rows_tables<OffT>(P, T, tInY.data(), tOutY.data(), tCy.data(), 0, 1);
+int replay_rows(const HpttProblem &P, const HpttTile &T, const Layout &L,
+                const std::vector<unsigned char> &tab, std::vector<uint8_t> &writes,
+                uint64_t *checked) {
+  const int vec = T.vec;
   const int esz = elem_bytes(P.dtype);
   const int J = hptt_jmax_rows(esz * vec);
   if (T.J1 > J) return 201;
-  if (T.TY * (2 * static_cast<int>(sizeof(OffT)) + 4) > T.smem_bytes) return 202;
-  if (vec > 1 && (P.sA[0] != 1 || P.sB[0] != 1)) return 203;
+  if (T.tab2_off < T.TY * static_cast<int>(sizeof(OffT))) return 202;
+  if (T.table_bytes < T.tab2_off + T.TY * static_cast<int>(sizeof(OffT))) return 203;
+  if (vec > 1 && (P.sA[0] != 1 || P.sB[0] != 1)) return 204;
+  const OffT *tabA = reinterpret_cast<const OffT *>(tab.data());
+  const OffT *tabB = reinterpret_cast<const OffT *>(tab.data() + T.tab2_off);
   for (uint32_t tile = 0; tile < T.num_tiles; ++tile) {
     const TileOrigin o = tile_origin(P, T, tile);
+    const int limY = rows_limit_y(T, o);
     for (int t = 0; t < T.nt; ++t) {
-      const RowThread<OffT> s = rows_thread<OffT>(T, t);
+      const RowThread s = rows_thread(T, t);
       if (!s.active) continue;
       const int64_t col = static_cast<int64_t>(s.e) * vec;
-      const bool col_ok = o.interior || col < o.remX;
+      if (col >= o.remX) continue;
       for (int j = 0; j < J; ++j) {
         const int y = s.y0 + j * T.R1;
-        if (!(j < T.J1 && y < T.TY && col_ok && (o.interior || tCy[y] < o.remY))) continue;
-        const int64_t a0 = o.bA + col * P.sA[0] + static_cast<int64_t>(tInY[y]);
-        const int64_t b0 = o.bB + col * P.sB[0] + static_cast<int64_t>(tOutY[y]);
-        if (vec > 1 && ((a0 % vec) != 0 || (b0 % vec) != 0)) return 204;
+        if (!(j < T.J1 && y < limY)) continue;
+        if (y < 0 || y >= T.TY) return 205;
+        const int64_t a0 = o.bA + col * P.sA[0] + static_cast<int64_t>(tabA[y]);
+        const int64_t b0 = o.bB + col * P.sB[0] + static_cast<int64_t>(tabB[y]);
+        if (vec > 1 && ((a0 % vec) != 0 || (b0 % vec) != 0)) return 206;
         for (int k = 0; k < vec; ++k) {
           const int64_t ia = a0 + k, ib = b0 + k;
-          if (ia < 0 || ia >= L.nA) return 205;
-          if (ib < 0 || ib >= L.nB) return 206;
-          if (map_a_to_b(L, ia) != ib) return 207;
-          if (writes[ib] != 0) return 208;
+          if (ia < 0 || ia >= L.nA) return 207;
+          if (ib < 0 || ib >= L.nB) return 208;
+          if (map_a_to_b(L, ia) != ib) return 209;
+          if (writes[ib] != 0) return 210;
           writes[ib] = 1;
           ++*checked;
         }
@@ -170,9 +179,6 @@ extern "C" int hptt_cuda_debug_check_indexing(int dtype, uint32_t rank, const ui
   if (st != ST_OK) return st;
   TileParams tp;
   if (max_vec_bytes > 0) tp.max_vec_bytes = max_vec_bytes;
-  HpttTile T;
-  st = choose_tile(P, tp, &T);
-  if (st != ST_OK) return st;
   Layout L;
   L.rank = static_cast<int>(rank);
   for (uint32_t d = 0; d < rank; ++d) {
@@ -189,18 +195,25 @@ extern "C" int hptt_cuda_debug_check_indexing(int dtype, uint32_t rank, const ui
     s *= L.out_outer[k];
   }
   L.nB = s;
-  std::vector<uint8_t> writes(static_cast<size_t>(L.nB), 0);
-  uint64_t n = 0;
-  int rc;
-  if (T.kind == KIND_TILE)
-    rc = T.big_offsets ? replay_tile<int64_t>(P, T, L, writes, &n)
-                       : replay_tile<uint32_t>(P, T, L, writes, &n);
-  else
-    rc = T.big_offsets ? replay_rows<int64_t>(P, T, L, T.vec, writes, &n)
-                       : replay_rows<uint32_t>(P, T, L, T.vec, writes, &n);
-  if (rc != 0) return 1000 + rc;
-  for (int64_t ib = 0; ib < L.nB; ++ib)
-    if (static_cast<bool>(writes[ib]) != b_is_inner(L, ib)) return 1300;
-  if (checked) *checked = n;
+  for (int update = 0; update < 2; ++update) {
+    HpttTile T;
+    st = choose_tile(P, tp, update, &T);
+    if (st != ST_OK) return st;
+    std::vector<unsigned char> tab;
+    build_tables(P, T, &tab);
+    std::vector<uint8_t> writes(static_cast<size_t>(L.nB), 0);
+    uint64_t n = 0;
+    int rc;
+    if (T.kind == KIND_TILE)
+      rc = T.big_offsets ? replay_tile<int64_t>(P, T, L, tab, writes, &n)
+                         : replay_tile<uint32_t>(P, T, L, tab, writes, &n);
+    else
+      rc = T.big_offsets ? replay_rows<int64_t>(P, T, L, tab, writes, &n)
+                         : replay_rows<uint32_t>(P, T, L, tab, writes, &n);
+    if (rc != 0) return 1000 + rc;
+    for (int64_t ib = 0; ib < L.nB; ++ib)
+      if (static_cast<bool>(writes[ib]) != b_is_inner(L, ib)) return 1300;
+    if (checked) *checked = n;
+  }
   return 0;
 }

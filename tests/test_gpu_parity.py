@@ -83,7 +83,7 @@ def test_tiny_leading_extents(name, lead):
 @pytest.mark.parametrize("name", DTYPES)
 def test_outer_sizes(name):
     _check(name, [5, 6, 7], [2, 0, 1], 2.3, 4.2, io=[8, 6, 9])
-    _check(name, [5, 6, 7], [2, 0, 1], 1.0, 0.0, oo=[9, 5, 10])
+    _check(name, [5, 6, 7], [2, 0, 1], 1.0, 0.0, oo=[9, 8, 10])
     _check(name, [5, 6, 7], [0, 2, 1], 2.3, 4.2, io=[6, 7, 7], oo=[7, 7, 8])
     _check(name, [64, 6, 7], [0, 1, 2], 2.3, 4.2, io=[66, 6, 7], oo=[65, 7, 7])
 

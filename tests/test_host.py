@@ -77,4 +77,4 @@ def test_tile_invariants_random(seed):
     if p["kind"] == "tile":
         assert p["W"] * p["TX"] <= 256 and p["W"] * p["TY"] <= 256
         assert p["LD"] >= p["W"] * p["TX"]
-        assert p["smem"] <= 48 * 1024
+        assert p["smem"] <= 227 * 1024  # opt-in shared memory per CTA on sm_100
