@@ -90,6 +90,9 @@ int replay_tile(const HpttProblem &P, const HpttTile &T, const Layout &L,
           if (ia < 0 || ia >= L.nA) return 109;
           slot[si] = ia;
         } else {
+          // the kernel re-reads this thread's first element of the tile
+          const int64_t ia0 = o.bA + th.inE;
+          if (ia0 < 0 || ia0 >= L.nA || map_a_to_b(L, ia0) < 0) return 117;
           slot[si] = -3;  // written, value unused
         }
       }
@@ -101,7 +104,12 @@ int replay_tile(const HpttProblem &P, const HpttTile &T, const Layout &L,
       for (int j = 0; j < J; ++j) {
         const int q = th.qs0 + j * T.R2;
         if (!(j < T.J2 && q < T.TX)) continue;
-        if (!(tabX[q].c < o.remX)) continue;
+        if (!(tabX[q].c < o.remX)) {
+          // the B prefetch re-reads this thread's first store element
+          const int64_t ib0 = o.bB + th.outE2;
+          if (ib0 < 0 || ib0 >= L.nB || !b_is_inner(L, ib0)) return 118;
+          continue;
+        }
         const int64_t si = static_cast<int64_t>(th.sme2) + static_cast<int64_t>(q) * T.W;
         if (si < 0 || si >= smem_elems) return 112;
         const int64_t ia = slot[si];
