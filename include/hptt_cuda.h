@@ -161,6 +161,45 @@ int hptt_cuda_debug_check_indexing(int dtype, uint32_t rank, const uint32_t *in_
                                    const uint32_t *out_outer, int max_vec_bytes,
                                    uint64_t *checked);
 
+/* Size of the fixed device array hptt_cuda_transpose_noalloc keeps its
+ * offset tables in (one array per GPU, held until the process exits). */
+#define HPTT_NOALLOC_TABLE_BYTES 65536
+
+/*
+ * One transpose that allocates no device memory.
+ *
+ * No counterpart in the reference.  hptt_cuda_plan_create keeps a plan's
+ * offset tables (a few KB) in device memory it obtains with cudaMalloc.
+ * Callers that cannot allocate device memory when they transpose -- code
+ * recording work while a stream is being captured, frameworks whose device
+ * memory comes only from their own pool or arena, jobs held to a fixed
+ * memory budget -- use this call instead.  It plans the transpose on the
+ * host, copies the tables into a fixed HPTT_NOALLOC_TABLE_BYTES array
+ * compiled into the library, and enqueues the same kernel on `stream`
+ * (cudaStream_t as void*, NULL = the legacy default stream).  It never calls
+ * cudaMalloc, cudaFree or another device allocator.
+ *
+ * Arguments mean what they mean for hptt_cuda_plan_create; in/out are device
+ * pointers the caller owns.  Returns HPTT_ERR_TOO_LARGE when this problem's
+ * tables would not fit the array.
+ *
+ * The array is shared by every call in the process on that GPU and keeps
+ * the last call's tables: calls that can run at the same time on the GPU
+ * (different streams, several host threads) race on it and must be
+ * serialised by the caller; calls on one stream are ordered.  The first call
+ * on each device looks the array's address up (a one-time set-up); make
+ * that first call before any stream capture begins.
+ */
+int hptt_cuda_transpose_noalloc(int dtype, uint32_t rank, const uint32_t *in_size,
+                                const uint32_t *perm, const uint32_t *in_outer,
+                                const uint32_t *out_outer, const double *alpha,
+                                const double *beta, int complex_scalars, const void *in,
+                                void *out, void *stream);
+
+/* HPTT_NOALLOC_TABLE_BYTES as compiled into the library.  No counterpart in
+ * the reference. */
+size_t hptt_cuda_noalloc_table_bytes(void);
+
 /* Static text for a status code. */
 const char *hptt_cuda_status_string(int status);
 
