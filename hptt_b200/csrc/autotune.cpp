@@ -36,12 +36,8 @@ std::string gpu_name() {
 
 const char *env_path() { return std::getenv("HPTT_B200_TUNE_CACHE"); }
 
-void ensure_loaded() {
-  if (g_loaded) return;
-  g_loaded = true;
-  const char *p = env_path();
-  if (!p) return;
-  std::ifstream f(p);
+// Cache file: one line per key, "key|run vmin smem rows_min y_first".
+void read_cache_stream(std::istream &f) {
   std::string line;
   while (std::getline(f, line)) {
     const auto bar = line.find('|');
@@ -49,9 +45,18 @@ void ensure_loaded() {
     std::istringstream v(line.substr(bar + 1));
     TileParams tp;
     if (v >> tp.run_bytes >> tp.vmin_bytes >> tp.smem_bytes >> tp.rows_min_bytes >>
-        tp.ctas_per_sm)
+        tp.y_first)
       g_cache[line.substr(0, bar)] = tp;
   }
+}
+
+void ensure_loaded() {
+  if (g_loaded) return;
+  g_loaded = true;
+  const char *p = env_path();
+  if (!p) return;
+  std::ifstream f(p);
+  read_cache_stream(f);
 }
 
 int write_cache(const char *path) {
@@ -60,19 +65,21 @@ int write_cache(const char *path) {
   for (const auto &kv : g_cache)
     f << kv.first << "|" << kv.second.run_bytes << " " << kv.second.vmin_bytes << " "
       << kv.second.smem_bytes << " " << kv.second.rows_min_bytes << " "
-      << kv.second.ctas_per_sm << "\n";
+      << kv.second.y_first << "\n";
   return ST_OK;
 }
 
+// Candidate tile parameters: which side is chosen first, the contiguous run
+// wanted on each side, and the minimum tile volume.
 std::vector<TileParams> candidates() {
   std::vector<TileParams> c;
-  for (int run : {256, 128, 512})
-    for (int vmin : {16384, 8192, 32768})
-      for (int cps : {0, 4, 2}) {
+  for (int yf : {0, 1})
+    for (int run : {256, 128, 512})
+      for (int vmin : {16384, 8192}) {
         TileParams tp;
+        tp.y_first = yf;
         tp.run_bytes = run;
         tp.vmin_bytes = vmin;
-        tp.ctas_per_sm = cps;
         c.push_back(tp);
       }
   return c;
@@ -178,16 +185,7 @@ int autotune_cache_load(const char *path) {
   }
   std::ifstream f(path);
   if (!f) return ST_ALLOC;
-  std::string line;
-  while (std::getline(f, line)) {
-    const auto bar = line.find('|');
-    if (bar == std::string::npos) continue;
-    std::istringstream v(line.substr(bar + 1));
-    TileParams tp;
-    if (v >> tp.run_bytes >> tp.vmin_bytes >> tp.smem_bytes >> tp.rows_min_bytes >>
-        tp.ctas_per_sm)
-      g_cache[line.substr(0, bar)] = tp;
-  }
+  read_cache_stream(f);
   g_loaded = true;
   return ST_OK;
 }

@@ -257,8 +257,20 @@ int hptt_cuda_plan_set_coef(hptt_cuda_plan_t plan, const double *alpha,
   Plan *p = reinterpret_cast<Plan *>(plan);
   if (!plan_valid(p)) return HPTT_ERR_HANDLE;
   if (!alpha || !beta) return HPTT_ERR_SIZE_VALUE;
+  const int old_update = p->args.update;
   set_scalars(&p->args, alpha, beta, complex_scalars);
-  return HPTT_OK;
+  if (p->args.update == old_update) return HPTT_OK;
+  // Whether B is read changes the tile shape (per-thread iterations): plan
+  // the tiles again on the plan's device.
+  int cur = 0;
+  if (cudaGetDevice(&cur) != cudaSuccess) return HPTT_ERR_NO_DEVICE;
+  if (cur != p->device && cudaSetDevice(p->device) != cudaSuccess) return HPTT_ERR_CUDA;
+  TileParams params;
+  if (!autotune_cache_lookup(p, &params)) params = TileParams();
+  int st = plan_tiles(p, params);
+  if (st != ST_OK) st = plan_tiles(p, TileParams());
+  if (cur != p->device) cudaSetDevice(cur);
+  return st;
 }
 
 int hptt_cuda_plan_bytes(hptt_cuda_plan_t plan, uint64_t *bytes) {

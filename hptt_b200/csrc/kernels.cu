@@ -13,16 +13,18 @@ namespace {
 constexpr int kNT = 256;
 
 // One CTA per tile.  The arguments live in the parameter space
-// (__grid_constant__) and are read through a const reference.
-template <typename E, int MODE, bool UPD, typename OffT>
-__global__ void __launch_bounds__(kNT) k_tile(const __grid_constant__ HpttArgs args) {
+// (__grid_constant__) and are read through a const reference.  Register
+// budgets: 6 resident CTAs per SM for the copy/scale tiles (the shared-memory
+// limit at 32 KB a tile), 4 when B is read too.
+template <typename E, int MODE, bool UPD, typename OffT, bool LX, bool LY>
+__global__ void __launch_bounds__(kNT, UPD ? 4 : 6) k_tile(const __grid_constant__ HpttArgs args) {
   extern __shared__ __align__(16) unsigned char smem[];
   const Scal sc{args.alpha[0], args.alpha[1], args.beta[0], args.beta[1]};
   const Op<E, MODE, UPD> op(sc);
-  tile_one<E, MODE, UPD, OffT>(args.p, args.t, static_cast<const E *>(args.A),
-                               static_cast<E *>(args.B),
-                               static_cast<const unsigned char *>(args.tables), op,
-                               reinterpret_cast<E *>(smem), blockIdx.x);
+  tile_one<E, MODE, UPD, OffT, LX, LY>(args.p, args.t, static_cast<const E *>(args.A),
+                                       static_cast<E *>(args.B),
+                                       static_cast<const unsigned char *>(args.tables), op,
+                                       reinterpret_cast<E *>(smem), blockIdx.x);
 }
 
 template <typename E, int MODE, bool UPD, typename OffT, int VEC>
@@ -38,9 +40,16 @@ __global__ void __launch_bounds__(kNT) k_rows(const __grid_constant__ HpttArgs a
 // ---------------------------------------------------------------------------
 // dispatch
 // ---------------------------------------------------------------------------
+// 64-bit table offsets only on the general path; single-dim sides compute
+// their offsets in 64 bits anyway.
 template <typename E, int MODE, bool UPD, typename OffT>
-const void *pick_tile() {
-  return reinterpret_cast<const void *>(&k_tile<E, MODE, UPD, OffT>);
+const void *pick_tile(const HpttTile &t) {
+  if (sizeof(OffT) == 8) return reinterpret_cast<const void *>(&k_tile<E, MODE, UPD, int64_t, false, false>);
+  const bool lx = t.nx <= 1, ly = t.ny <= 1;
+  if (lx && ly) return reinterpret_cast<const void *>(&k_tile<E, MODE, UPD, uint32_t, true, true>);
+  if (lx) return reinterpret_cast<const void *>(&k_tile<E, MODE, UPD, uint32_t, true, false>);
+  if (ly) return reinterpret_cast<const void *>(&k_tile<E, MODE, UPD, uint32_t, false, true>);
+  return reinterpret_cast<const void *>(&k_tile<E, MODE, UPD, uint32_t, false, false>);
 }
 
 template <typename E, int MODE, bool UPD, typename OffT>
@@ -58,7 +67,7 @@ template <typename E, int MODE, bool UPD>
 const void *pick_off(const HpttTile &t, int vec) {
   const int vb = vec * static_cast<int>(sizeof(E));
   if (t.kind == KIND_TILE)
-    return t.big_offsets ? pick_tile<E, MODE, UPD, int64_t>() : pick_tile<E, MODE, UPD, uint32_t>();
+    return t.big_offsets ? pick_tile<E, MODE, UPD, int64_t>(t) : pick_tile<E, MODE, UPD, uint32_t>(t);
   return t.big_offsets ? pick_rows<E, MODE, UPD, int64_t>(vb) : pick_rows<E, MODE, UPD, uint32_t>(vb);
 }
 

@@ -154,6 +154,18 @@ HPTT_HD inline int rows_limit_y(const HpttTile &T, const TileOrigin &o) {
   return o.remY * T.py;
 }
 
+// n / d with the planner's multiply-high constants (mul == 0: d == 1);
+// exact for n < 2^31.
+HPTT_HD inline int fast_div(int n, uint32_t mul, int shr) {
+  return mul ? static_cast<int>(umulhi32(static_cast<uint32_t>(n), mul) >> shr) : n;
+}
+
+// Iterations j >= 0 with q0 + j * R < lim (R > 0): ceil((lim - q0) / R), or 0.
+HPTT_HD inline int valid_iters(int lim, int q0, uint32_t mul, int shr, int R) {
+  return lim > q0 ? fast_div(lim - q0 + R - 1, mul, shr) : 0;
+}
+
+
 // ---------------------------------------------------------------------------
 // One tile through shared memory (one CTA).
 //
@@ -165,33 +177,49 @@ HPTT_HD inline int rows_limit_y(const HpttTile &T, const TileOrigin &o) {
 // input-contiguous runs -- plus, when B is read, the B elements it combines
 // later.  Store phase: thread (e2, qs0) writes columns q = qs0 + j*R2 of its
 // element e2 -- output-contiguous runs.
+//
+// LX / LY: the X (Y) side has at most one dim, so slot q IS that dim's
+// coordinate: offset q * stride and validity q < remaining extent, with no
+// table read (the tables hold exactly these values; the CPU replay checks
+// that).
 // ---------------------------------------------------------------------------
-template <typename E, int MODE, bool UPD, typename OffT>
+template <typename E, int MODE, bool UPD, typename OffT, bool LX, bool LY>
 __device__ __forceinline__ void tile_one(const HpttProblem &P, const HpttTile &T,
                                          const E *__restrict__ A, E *__restrict__ B,
                                          const unsigned char *__restrict__ tables,
                                          const Op<E, MODE, UPD> &op, E *sdata, uint32_t tile) {
-  constexpr int J = hptt_jmax_tile(sizeof(E));
+  constexpr int J = hptt_jmax_tile(sizeof(E), UPD);
   using Ent = HpttTabEnt<OffT>;
   const Ent *__restrict__ tabY = reinterpret_cast<const Ent *>(tables);
   const Ent *__restrict__ tabX = reinterpret_cast<const Ent *>(tables + T.tab2_off);
   const HpttThr th = reinterpret_cast<const HpttThr *>(tables + T.thr_off)[threadIdx.x];
   const TileOrigin o = tile_origin(P, T, tile);
-  const int LD = T.LD, W = T.W, R1 = T.R1, R2 = T.R2, J1 = T.J1, J2 = T.J2;
+  const int LD = T.LD, W = T.W, R1 = T.R1, R2 = T.R2;
   const int TX = T.TX, TY = T.TY;
-  const bool ld_ok = (th.active & 1) && th.cxe < o.remX;
-  const bool st_ok = (th.active & 2) && th.cye2 < o.remY;
+  // iterations with a row (column) slot inside the tile -- and, on a
+  // single-dim side, inside the tensor
+  int nL = (th.cxe < o.remX) ? th.nld : 0;
+  int nS = (th.cye2 < o.remY) ? th.nst : 0;
+  if (LY && T.yc >= 0 && o.remY < TY)
+    nL = min(nL, valid_iters(o.remY, th.q0, T.r1_mul, T.r1_shr, R1));
+  if (LX && T.xc >= 0 && o.remX < TX)
+    nS = min(nS, valid_iters(o.remX, th.qs0, T.r2_mul, T.r2_shr, R2));
+  // single-dim sides: in-tile offsets fit 32 bits (OffT is 32-bit there)
+  const int sY = (LY && T.ny == 1) ? static_cast<int>(P.sA[T.yd[0]]) : 0;
+  const int sX = (LX && T.nx == 1) ? static_cast<int>(P.sB[T.xd[0]]) : 0;
 
   // Loads never branch on table contents: an out-of-range row or column
   // re-reads the tile's own first element (always inside: its coordinates
   // along the chunked dims are 0), so all loads issue back to back.
   E v[J];
-  if (ld_ok) {
-    const E *src = A + o.bA + th.inE;
+  const E *src = A + o.bA + th.inE;
 #pragma unroll
-    for (int j = 0; j < J; ++j) {
+  for (int j = 0; j < J; ++j) {
+    if (j < nL) {
       const int q = th.q0 + j * R1;
-      if (j < J1 && q < TY) {
+      if (LY) {
+        v[j] = __ldg(src + q * sY);
+      } else {
         const Ent en = tabY[q];
         v[j] = __ldg(src + (en.c < o.remY ? en.off : OffT(0)));
       }
@@ -199,37 +227,45 @@ __device__ __forceinline__ void tile_one(const HpttProblem &P, const HpttTile &T
   }
   E *dst = B + o.bB + th.outE2;
   E bv[J];
-  if (UPD && st_ok) {
+  if (UPD) {
 #pragma unroll
     for (int j = 0; j < J; ++j) {
-      const int q = th.qs0 + j * R2;
-      if (j < J2 && q < TX) {
-        const Ent en = tabX[q];
-        bv[j] = dst[en.c < o.remX ? en.off : OffT(0)];
+      if (j < nS) {
+        const int q = th.qs0 + j * R2;
+        if (LX) {
+          bv[j] = dst[q * sX];
+        } else {
+          const Ent en = tabX[q];
+          bv[j] = dst[en.c < o.remX ? en.off : OffT(0)];
+        }
       }
     }
   }
-  if (ld_ok) {
+  {
     E *s = sdata + th.q0 * LD + th.sme;
 #pragma unroll
-    for (int j = 0; j < J; ++j) {
-      const int q = th.q0 + j * R1;
-      if (j < J1 && q < TY) s[j * R1 * LD] = v[j];
-    }
+    for (int j = 0; j < J; ++j)
+      if (j < nL) s[j * R1 * LD] = v[j];
   }
   __syncthreads();
-  if (st_ok) {
-    const E *s = sdata + th.sme2 + th.qs0 * W;
+  const E *s = sdata + th.sme2 + th.qs0 * W;
 #pragma unroll
-    for (int j = 0; j < J; ++j) {
+  for (int j = 0; j < J; ++j) {
+    if (j < nS) {
       const int q = th.qs0 + j * R2;
-      if (j < J2 && q < TX) {
+      bool ok = true;
+      int64_t off;
+      if (LX) {
+        off = q * sX;
+      } else {
         const Ent en = tabX[q];
-        if (en.c < o.remX) {
-          const E a = s[j * R2 * W];
-          const E r = op(a, UPD ? bv[j] : a);
-          if (UPD) dst[en.off] = r; else __stcs(dst + en.off, r);
-        }
+        ok = en.c < o.remX;
+        off = static_cast<int64_t>(en.off);
+      }
+      if (ok) {
+        const E a = s[j * R2 * W];
+        const E r = op(a, UPD ? bv[j] : a);
+        if (UPD) dst[off] = r; else __stcs(dst + off, r);
       }
     }
   }
@@ -250,26 +286,26 @@ __device__ __forceinline__ void rows_one(const HpttProblem &P, const HpttTile &T
   const TileOrigin o = tile_origin(P, T, tile);
   const int64_t col = static_cast<int64_t>(s.e) * VEC;
   if (col >= o.remX) return;
-  const int limY = rows_limit_y(T, o);
+  const int n = min(T.J1, valid_iters(rows_limit_y(T, o), s.y0, T.r1_mul, T.r1_shr, T.R1));
   const OffT *__restrict__ tabA = reinterpret_cast<const OffT *>(tables);
   const OffT *__restrict__ tabB = reinterpret_cast<const OffT *>(tables + T.tab2_off);
   const E *src = A + o.bA + col * P.sA[0];
   E *dst = B + o.bB + col * P.sB[0];
-  const int R1 = T.R1, J1 = T.J1;
+  const int R1 = T.R1;
   Vec<E, VEC> av[J];
   Vec<E, VEC> bv[J];
 #pragma unroll
   for (int j = 0; j < J; ++j) {
-    const int y = s.y0 + j * R1;
-    if (j < J1 && y < limY) {
+    if (j < n) {
+      const int y = s.y0 + j * R1;
       av[j] = ld_vec<E, VEC>(src + __ldg(tabA + y));
       if (UPD) bv[j] = ld_vec_rw<E, VEC>(dst + __ldg(tabB + y));
     }
   }
 #pragma unroll
   for (int j = 0; j < J; ++j) {
-    const int y = s.y0 + j * R1;
-    if (j < J1 && y < limY) {
+    if (j < n) {
+      const int y = s.y0 + j * R1;
       Vec<E, VEC> r;
 #pragma unroll
       for (int k = 0; k < VEC; ++k) r.v[k] = op(av[j].v[k], UPD ? bv[j].v[k] : av[j].v[k]);

@@ -261,6 +261,12 @@ HpttThr tile_thread_consts(const HpttProblem &p, const HpttTile &t, const TileMa
               static_cast<int64_t>(w) * p.sB[0];
     h.sme2 = m.qrow[y] * t.LD + w;
   }
+  auto count = [](int lim, int q0, int R, int J) {
+    if (q0 >= lim) return 0;
+    return std::min(J, (lim - q0 + R - 1) / R);
+  };
+  h.nld = static_cast<int16_t>(ld ? count(t.TY, h.q0, t.R1, t.J1) : 0);
+  h.nst = static_cast<int16_t>(st ? count(t.TX, h.qs0, t.R2, t.J2) : 0);
   return h;
 }
 
@@ -335,8 +341,8 @@ struct Side {
 };
 
 bool shape_ok(const TileParams &tp, int64_t W, const Side &X, const Side &Y,
-              int sz) {
-  const int kJMax = hptt_jmax_tile(sz);
+              int sz, int update) {
+  const int kJMax = hptt_jmax_tile(sz, update);
   const int64_t TX = X.prod(), TY = Y.prod();
   const int64_t RW = W * TX, WTY = W * TY;
   if (RW > tp.nt || WTY > tp.nt) return false;
@@ -344,6 +350,22 @@ bool shape_ok(const TileParams &tp, int64_t W, const Side &X, const Side &Y,
   if (cdiv(TY, R1) > kJMax || cdiv(TX, R2) > kJMax) return false;
   if (RW * TY * sz > tp.smem_bytes) return false;
   return true;
+}
+
+// Division by a run-time constant d as multiply-high and shift, exact for
+// dividends below 2^31: with l = ceil(log2 d) and p = 31 + l,
+// m = ceil(2^p / d) and n / d = (n * m) >> p.  mul = 0 encodes d == 1.
+void fast_div_magic(uint32_t d, uint32_t *mul, int32_t *shr) {
+  if (d <= 1) {
+    *mul = 0;
+    *shr = 0;
+    return;
+  }
+  int l = 0;
+  while ((1ull << l) < d) ++l;
+  const int pw = 31 + l;
+  *mul = static_cast<uint32_t>(((1ull << pw) + d - 1) / d);
+  *shr = pw - 32;
 }
 
 void finish_grid(const HpttProblem &p, HpttTile *t, const int64_t *tile_ext,
@@ -368,22 +390,15 @@ void finish_grid(const HpttProblem &p, HpttTile *t, const int64_t *tile_ext,
   for (int d = 0; d < p.rank; ++d)
     if (!used[d]) add(d);
   t->num_tiles = tiles > 0x7fffffffULL ? 0 : static_cast<uint32_t>(tiles);
-  // Division by a run-time constant as multiply-high and shift, exact for
-  // dividends below 2^31 (tile indices are): with l = ceil(log2 d) and
-  // p = 31 + l, m = ceil(2^p / d) and n / d = (n * m) >> p.
-  for (int g = 0; g < t->ng; ++g) {
-    const uint32_t d = t->gcnt[g];
-    if (d <= 1) {
-      t->gmul[g] = 0;
-      t->gshr[g] = 0;
-      continue;
-    }
-    int l = 0;
-    while ((1ull << l) < d) ++l;
-    const int pw = 31 + l;
-    t->gmul[g] = static_cast<uint32_t>(((1ull << pw) + d - 1) / d);
-    t->gshr[g] = pw - 32;
-  }
+  for (int g = 0; g < t->ng; ++g) fast_div_magic(t->gcnt[g], &t->gmul[g], &t->gshr[g]);
+}
+
+// The fast divisions by R1/R2.  (Tile origins are decoded on the device: a
+// per-tile origin table was measured slower -- every CTA's first loads then
+// wait on a cold read of its own entry.)
+void finish_tables(HpttTile *t) {
+  fast_div_magic(static_cast<uint32_t>(t->R1 > 0 ? t->R1 : 1), &t->r1_mul, &t->r1_shr);
+  fast_div_magic(static_cast<uint32_t>(t->R2 > 0 ? t->R2 : 1), &t->r2_mul, &t->r2_shr);
 }
 
 int choose_rows(const HpttProblem &p, const TileParams &tp, HpttTile *t) {
@@ -453,6 +468,7 @@ int choose_rows(const HpttProblem &p, const TileParams &tp, HpttTile *t) {
   t->tab2_off = (t->TY * off + 15) & ~15;
   t->thr_off = t->tab2_off + ((t->TY * off + 15) & ~15);
   t->table_bytes = t->thr_off;
+  finish_tables(t);
   return t->num_tiles ? ST_OK : ST_TOO_LARGE;
 }
 
@@ -478,10 +494,16 @@ int choose_tile(const HpttProblem &p, const TileParams &tp, int update, HpttTile
   if (common) in_tile[0] = true;
 
   Side X, Y;
-  {
+  // X: input-order dims (stopping at the output's leading dim, or skipping
+  // dims Y already holds when Y is chosen first); Y: output-order dims.
+  auto pick_x = [&]() {
     int64_t prod = W;
     for (int d = si; d < r; ++d) {
-      if (d == p.perm[so]) break;
+      if (in_tile[d]) {
+        if (tp.y_first) continue;
+        break;
+      }
+      if (!tp.y_first && d == p.perm[so]) break;
       const int64_t cap = tp.nt / prod;
       const int64_t tt = std::min({p.n[d], cdiv(target, prod), cap});
       if (tt < 1) break;
@@ -491,7 +513,9 @@ int choose_tile(const HpttProblem &p, const TileParams &tp, int update, HpttTile
       prod *= tt;
       if (tt < p.n[d] || prod >= target) break;
     }
-    prod = W;
+  };
+  auto pick_y = [&]() {
+    int64_t prod = W;
     for (int k = so; k < r; ++k) {
       const int d = p.perm[k];
       if (in_tile[d]) break;
@@ -504,9 +528,16 @@ int choose_tile(const HpttProblem &p, const TileParams &tp, int update, HpttTile
       prod *= tt;
       if (tt < p.n[d] || prod >= target) break;
     }
+  };
+  if (tp.y_first) {
+    pick_y();
+    pick_x();
+  } else {
+    pick_x();
+    pick_y();
   }
   // shrink until the shape fits the thread mapping (the larger side first)
-  for (int guard = 0; guard < 4096 && !shape_ok(tp, W, X, Y, sz); ++guard) {
+  for (int guard = 0; guard < 4096 && !shape_ok(tp, W, X, Y, sz, update); ++guard) {
     Side *S = (X.prod() >= Y.prod()) ? &X : &Y;
     if (S->d.empty()) S = (S == &X) ? &Y : &X;
     if (S->d.empty()) break;
@@ -552,7 +583,7 @@ int choose_tile(const HpttProblem &p, const TileParams &tp, int update, HpttTile
         const int64_t old = tt;
         const int64_t want = std::min<int64_t>(p.n[d], std::max<int64_t>(old + 1, old * 2));
         tt = want;
-        while (tt > old && !shape_ok(tp, W, X, Y, sz)) --tt;
+        while (tt > old && !shape_ok(tp, W, X, Y, sz, update)) --tt;
         if (tt > old) grown = true; else tt = old;
       } else {
         if (!S.d.empty() && S.t.back() < p.n[S.d.back()]) continue;
@@ -564,8 +595,8 @@ int choose_tile(const HpttProblem &p, const TileParams &tp, int update, HpttTile
         int64_t &tt = S.t.back();
         const int64_t want = std::min<int64_t>(p.n[d], cdiv(vmin, vol()));
         tt = std::max<int64_t>(1, want);
-        while (tt > 1 && !shape_ok(tp, W, X, Y, sz)) --tt;
-        if (tt > 1 && shape_ok(tp, W, X, Y, sz)) {
+        while (tt > 1 && !shape_ok(tp, W, X, Y, sz, update)) --tt;
+        if (tt > 1 && shape_ok(tp, W, X, Y, sz, update)) {
           grown = true;
         } else {
           S.d.pop_back();
@@ -587,12 +618,12 @@ int choose_tile(const HpttProblem &p, const TileParams &tp, int update, HpttTile
     const int64_t old = tt;
     if (2 * n <= 3 * tt) {
       tt = n;
-      if (shape_ok(tp, W, X, Y, sz)) continue;
+      if (shape_ok(tp, W, X, Y, sz, update)) continue;
       tt = old;
     }
     tt = cdiv(n, cdiv(n, old));
   }
-  if (!shape_ok(tp, W, X, Y, sz)) return ST_TOO_LARGE;
+  if (!shape_ok(tp, W, X, Y, sz, update)) return ST_TOO_LARGE;
 
   t->W = static_cast<int32_t>(W);
   t->nx = static_cast<int32_t>(X.d.size());
@@ -655,13 +686,13 @@ int choose_tile(const HpttProblem &p, const TileParams &tp, int update, HpttTile
   }
   t->big_offsets = (maxA >= 0x7fffffffLL || maxB >= 0x7fffffffLL);
   const int off = t->big_offsets ? 8 : 4;
-  (void)update;
   t->smem_bytes = (t->TY * t->LD * sz + 15) & ~15;
   auto a16 = [](int x) { return (x + 15) & ~15; };
   const int ent = 2 * off;  // sizeof(HpttTabEnt<OffT>)
   t->tab2_off = a16(t->TY * ent);
   t->thr_off = t->tab2_off + a16(t->TX * ent);
   t->table_bytes = t->thr_off + t->nt * static_cast<int>(sizeof(HpttThr));
+  finish_tables(t);
   return t->num_tiles ? ST_OK : ST_TOO_LARGE;
 }
 

@@ -39,6 +39,7 @@ struct TileParams {
   int rows_min_bytes = 512;  // shared stride-1 run long enough for KIND_ROWS
   int ctas_per_sm = 0;     // 0: as many as fit
   int max_vec_bytes = 16;  // widest vector access (KIND_ROWS)
+  int y_first = 0;         // choose the output-side dims before the input side
 };
 
 // Reference argument guard (src/hptt.cc:25-56) plus the one check the

@@ -55,11 +55,11 @@ bool b_is_inner(const Layout &L, int64_t ib) {
 }
 
 template <typename OffT>
-int replay_tile(const HpttProblem &P, const HpttTile &T, const Layout &L,
+int replay_tile(const HpttProblem &P, const HpttTile &T, int update, const Layout &L,
                 const std::vector<unsigned char> &tab, std::vector<uint8_t> &writes,
                 uint64_t *checked) {
   const int esz = elem_bytes(P.dtype);
-  const int J = hptt_jmax_tile(esz);
+  const int J = hptt_jmax_tile(esz, update);
   if (T.J1 > J || T.J2 > J) return 101;
   if (T.smem_bytes < T.TY * T.LD * esz) return 102;
   using Ent = HpttTabEnt<OffT>;
@@ -70,18 +70,40 @@ int replay_tile(const HpttProblem &P, const HpttTile &T, const Layout &L,
   const Ent *tabY = reinterpret_cast<const Ent *>(tab.data());
   const Ent *tabX = reinterpret_cast<const Ent *>(tab.data() + T.tab2_off);
   const HpttThr *thr = reinterpret_cast<const HpttThr *>(tab.data() + T.thr_off);
+  // Single-dim sides skip the tables in the kernel (offset q * stride,
+  // coordinate q along the chunked dim): the tables must hold exactly that,
+  // so replaying the tables replays those kernels too.
+  if (T.ny <= 1) {
+    const int64_t sY = T.ny == 1 ? P.sA[T.yd[0]] : 0;
+    for (int q = 0; q < T.TY; ++q)
+      if (static_cast<int64_t>(tabY[q].off) != q * sY || tabY[q].c != (T.yc >= 0 ? q : 0))
+        return 119;
+  }
+  if (T.nx <= 1) {
+    const int64_t sX = T.nx == 1 ? P.sB[T.xd[0]] : 0;
+    for (int q = 0; q < T.TX; ++q)
+      if (static_cast<int64_t>(tabX[q].off) != q * sX || tabX[q].c != (T.xc >= 0 ? q : 0))
+        return 120;
+  }
   const int64_t smem_elems = static_cast<int64_t>(T.TY) * T.LD;
   std::vector<int64_t> slot(smem_elems);
+  // the kernel's single-dim-side variants (kernels.cu: pick_tile)
+  const bool ly = !T.big_offsets && T.ny <= 1, lx = !T.big_offsets && T.nx <= 1;
   for (uint32_t tile = 0; tile < T.num_tiles; ++tile) {
     const TileOrigin o = tile_origin(P, T, tile);
     std::fill(slot.begin(), slot.end(), -1);
-    // load phase: every in-range slot is written (garbage when invalid)
+    // load phase, with the kernel's iteration counts
     for (int t = 0; t < T.nt; ++t) {
       const HpttThr &th = thr[t];
-      if (!((th.active & 1) && th.cxe < o.remX)) continue;
+      int nL = (th.cxe < o.remX) ? th.nld : 0;
+      if (ly && T.yc >= 0 && o.remY < T.TY)
+        nL = std::min(nL, valid_iters(o.remY, th.q0, T.r1_mul, T.r1_shr, T.R1));
+      if (nL > 0 && !(th.active & 1)) return 124;
       for (int j = 0; j < J; ++j) {
+        if (!(j < nL)) continue;
         const int q = th.q0 + j * T.R1;
-        if (!(j < T.J1 && q < T.TY)) continue;
+        if (!(j < T.J1 && q < T.TY)) return 125;
+        if (ly && !(tabY[q].c < o.remY)) return 121;
         const int64_t si = static_cast<int64_t>(q) * T.LD + th.sme;
         if (si < 0 || si >= smem_elems) return 108;
         if (slot[si] >= 0 || slot[si] == -3) return 110;  // two writers of one slot
@@ -100,10 +122,15 @@ int replay_tile(const HpttProblem &P, const HpttTile &T, const Layout &L,
     // store phase (and the B reads of the load phase, same addresses)
     for (int t = 0; t < T.nt; ++t) {
       const HpttThr &th = thr[t];
-      if (!((th.active & 2) && th.cye2 < o.remY)) continue;
+      int nS = (th.cye2 < o.remY) ? th.nst : 0;
+      if (lx && T.xc >= 0 && o.remX < T.TX)
+        nS = std::min(nS, valid_iters(o.remX, th.qs0, T.r2_mul, T.r2_shr, T.R2));
+      if (nS > 0 && !(th.active & 2)) return 126;
       for (int j = 0; j < J; ++j) {
+        if (!(j < nS)) continue;
         const int q = th.qs0 + j * T.R2;
-        if (!(j < T.J2 && q < T.TX)) continue;
+        if (!(j < T.J2 && q < T.TX)) return 127;
+        if (lx && !(tabX[q].c < o.remX)) return 122;
         if (!(tabX[q].c < o.remX)) {
           // the B prefetch re-reads this thread's first store element
           const int64_t ib0 = o.bB + th.outE2;
@@ -147,9 +174,11 @@ int replay_rows(const HpttProblem &P, const HpttTile &T, const Layout &L,
       if (!s.active) continue;
       const int64_t col = static_cast<int64_t>(s.e) * vec;
       if (col >= o.remX) continue;
+      const int n = std::min(T.J1, valid_iters(limY, s.y0, T.r1_mul, T.r1_shr, T.R1));
       for (int j = 0; j < J; ++j) {
         const int y = s.y0 + j * T.R1;
-        if (!(j < T.J1 && y < limY)) continue;
+        if (!(j < n)) continue;
+        if (!(j < T.J1 && y < limY)) return 212;
         if (y < 0 || y >= T.TY) return 205;
         const int64_t a0 = o.bA + col * P.sA[0] + static_cast<int64_t>(tabA[y]);
         const int64_t b0 = o.bB + col * P.sB[0] + static_cast<int64_t>(tabB[y]);
@@ -203,7 +232,11 @@ extern "C" int hptt_cuda_debug_check_indexing(int dtype, uint32_t rank, const ui
     s *= L.out_outer[k];
   }
   L.nB = s;
-  for (int update = 0; update < 2; ++update) {
+  // both tile strategies (input side first / output side first), both
+  // update settings
+  for (int variant = 0; variant < 4; ++variant) {
+    const int update = variant & 1;
+    tp.y_first = variant >> 1;
     HpttTile T;
     st = choose_tile(P, tp, update, &T);
     if (st != ST_OK) return st;
@@ -213,8 +246,8 @@ extern "C" int hptt_cuda_debug_check_indexing(int dtype, uint32_t rank, const ui
     uint64_t n = 0;
     int rc;
     if (T.kind == KIND_TILE)
-      rc = T.big_offsets ? replay_tile<int64_t>(P, T, L, tab, writes, &n)
-                         : replay_tile<uint32_t>(P, T, L, tab, writes, &n);
+      rc = T.big_offsets ? replay_tile<int64_t>(P, T, update, L, tab, writes, &n)
+                         : replay_tile<uint32_t>(P, T, update, L, tab, writes, &n);
     else
       rc = T.big_offsets ? replay_rows<int64_t>(P, T, L, tab, writes, &n)
                          : replay_rows<uint32_t>(P, T, L, tab, writes, &n);

@@ -155,6 +155,33 @@ def test_reset_data_set_coef_and_streams():
     assert "fused rank" in plan.describe()
 
 
+@pytest.mark.parametrize("name", ["f32", "f64"])
+def test_set_coef_switches_update(name):
+    """set_coef moving beta between zero and non-zero changes whether B is
+    read, and with it the tile shape: the plan re-plans its tiles."""
+    size, perm = [700, 90, 33], [2, 0, 1]
+    rng = np.random.default_rng(21)
+    n = int(np.prod(size))
+    a = seeded(rng, n, name)
+    b0 = seeded(rng, n, name)
+    da = torch.from_numpy(a).cuda()
+    db = torch.from_numpy(b0.copy()).cuda()
+    plan = h.create_plan(da, db, size, perm, 1.0, 0.0, 0)
+    before = plan.describe()
+    plan.set_coef(2.3, 4.2)
+    after = plan.describe()
+    db.copy_(torch.from_numpy(b0))
+    plan.exec()
+    plan.sync()
+    assert_same(db.cpu().numpy(), oracle_run(name, size, perm, 2.3, 4.2, a, b0), name,
+                f"update after set_coef ({before} -> {after})")
+    plan.set_coef(-0.5, 0.0)
+    plan.exec()
+    plan.sync()
+    assert_same(db.cpu().numpy(), oracle_run(name, size, perm, -0.5, 0.0, a, b0), name,
+                "scale after set_coef")
+
+
 def test_tuned_plan_matches():
     _check("f64", [96, 80, 12], [2, 0, 1], 2.3, 4.2)
     rng = np.random.default_rng(9)
