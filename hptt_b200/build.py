@@ -1,4 +1,5 @@
-"""Build libhptt_cuda.so in-tree for sm_100a with nvcc.
+"""Build libhptt_cuda.so in-tree for sm_100a with nvcc, and libhptt.so (the
+C++14 hptt::create_plan interface of include/hptt/hptt.h) over it with g++.
 
     python -m hptt_b200.build            # incremental
     python -m hptt_b200.build --clean    # from scratch
@@ -19,6 +20,9 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libhptt_cuda.so")
+CXX_SRC = os.path.join(HERE, "cxx")
+LIB_CXX = os.path.join(HERE, "libhptt.so")
+CXX = os.environ.get("CXX", "g++")
 INCLUDE = os.path.join(os.path.dirname(HERE), "include")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -75,7 +79,28 @@ def build(clean: bool = False, verbose: bool = False) -> str:
         if verbose:
             print(" ".join(cmd), flush=True)
         subprocess.run(cmd, check=True)
+    build_cxx(verbose)
     return LIB
+
+
+def build_cxx(verbose: bool = False) -> str:
+    """libhptt.so: hptt::create_plan and the create_trans_plan_impl_* factories
+    (C++14), linked against libhptt_cuda.so next to it."""
+    srcs = [os.path.join(CXX_SRC, f) for f in sorted(os.listdir(CXX_SRC)) if f.endswith(".cpp")]
+    deps = srcs + [LIB]
+    for root, _, files in os.walk(INCLUDE):
+        deps += [os.path.join(root, f) for f in files if f.endswith(".h")]
+    if os.path.exists(LIB_CXX) and os.path.getmtime(LIB_CXX) >= max(os.path.getmtime(d) for d in deps):
+        return LIB_CXX
+    cmd = [CXX, "-std=c++14", "-O2", "-fPIC", "-shared", "-Wall", "-I", INCLUDE] + srcs + \
+          ["-o", LIB_CXX, "-L", HERE, "-lhptt_cuda", "-Wl,-rpath,$ORIGIN"]
+    if verbose:
+        print(" ".join(cmd), flush=True)
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        sys.stderr.write(r.stdout + r.stderr)
+        raise RuntimeError("g++ failed on the C++ interface")
+    return LIB_CXX
 
 
 def main():

@@ -36,7 +36,8 @@ std::string gpu_name() {
 
 const char *env_path() { return std::getenv("HPTT_B200_TUNE_CACHE"); }
 
-// Cache file: one line per key, "key|run vmin smem rows_min y_first".
+// Cache file: one line per key, "key|run vmin smem rows_min y_first iters"
+// (a line without the last field keeps max_iters = 0).
 void read_cache_stream(std::istream &f) {
   std::string line;
   while (std::getline(f, line)) {
@@ -45,8 +46,10 @@ void read_cache_stream(std::istream &f) {
     std::istringstream v(line.substr(bar + 1));
     TileParams tp;
     if (v >> tp.run_bytes >> tp.vmin_bytes >> tp.smem_bytes >> tp.rows_min_bytes >>
-        tp.y_first)
+        tp.y_first) {
+      if (!(v >> tp.max_iters)) tp.max_iters = 0;
       g_cache[line.substr(0, bar)] = tp;
+    }
   }
 }
 
@@ -65,23 +68,26 @@ int write_cache(const char *path) {
   for (const auto &kv : g_cache)
     f << kv.first << "|" << kv.second.run_bytes << " " << kv.second.vmin_bytes << " "
       << kv.second.smem_bytes << " " << kv.second.rows_min_bytes << " "
-      << kv.second.y_first << "\n";
+      << kv.second.y_first << " " << kv.second.max_iters << "\n";
   return ST_OK;
 }
 
 // Candidate tile parameters: which side is chosen first, the contiguous run
-// wanted on each side, and the minimum tile volume.
-std::vector<TileParams> candidates() {
+// wanted on each side, the minimum tile volume, and the per-thread
+// iterations (the kernel's limit or half of it: smaller tiles, more CTAs).
+std::vector<TileParams> candidates(int elem_size) {
   std::vector<TileParams> c;
-  for (int yf : {0, 1})
-    for (int run : {256, 128, 512})
-      for (int vmin : {16384, 8192}) {
-        TileParams tp;
-        tp.y_first = yf;
-        tp.run_bytes = run;
-        tp.vmin_bytes = vmin;
-        c.push_back(tp);
-      }
+  for (int iters : {0, hptt_jmax_tile(elem_size) / 2})
+    for (int yf : {0, 1})
+      for (int run : {256, 128, 512})
+        for (int vmin : {16384, 8192}) {
+          TileParams tp;
+          tp.y_first = yf;
+          tp.run_bytes = run;
+          tp.vmin_bytes = vmin;
+          tp.max_iters = iters;
+          c.push_back(tp);
+        }
   return c;
 }
 
@@ -132,7 +138,7 @@ int autotune(Plan *p, double timeout, TileParams *best) {
   bool found = false;
   void *user_B = p->args.B;
   p->args.B = scratch;
-  for (const TileParams &tp : candidates()) {
+  for (const TileParams &tp : candidates(elem_bytes(p->args.p.dtype))) {
     if (st != ST_OK) break;
     if (timeout > 0) {
       const double el = std::chrono::duration<double>(std::chrono::steady_clock::now() - t_start).count();

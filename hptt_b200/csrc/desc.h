@@ -112,21 +112,19 @@ struct alignas(16) HpttThr {
   int32_t cxe;     // coordinate of e along the chunked X dim (0 if none)
   int32_t cye2;    // coordinate of e2 along the chunked Y dim (0 if none)
   int32_t active;  // bit 0: loads, bit 1: stores
-  int16_t nld;     // iterations j with row slot q0 + j*R1 < TY (0 if no loads)
-  int16_t nst;     // iterations j with column slot qs0 + j*R2 < TX (0 if no stores)
+  int32_t pad;
 };
 
 // Per-thread iterations of one phase, sized so every thread keeps about 64
-// (tile) or 128 (rows) bytes of loads in flight without spilling.  A 4-byte
-// tile that also reads B holds 8 A and 8 B values (16 + 16 would need about
-// 90 registers and halve the resident CTAs).
+// (tile) or 128 (rows) bytes of loads in flight without spilling.  (A tile
+// that also reads B keeps twice that: its B values are loaded alongside.)
 #ifdef __CUDACC__
 #define HPTT_HD __host__ __device__
 #else
 #define HPTT_HD
 #endif
-HPTT_HD constexpr int hptt_jmax_tile(int elem_bytes, int update) {
-  return elem_bytes >= 16 ? 4 : (elem_bytes >= 8 || update ? 8 : 16);
+HPTT_HD constexpr int hptt_jmax_tile(int elem_bytes) {
+  return elem_bytes >= 16 ? 4 : (elem_bytes >= 8 ? 8 : 16);
 }
 HPTT_HD constexpr int hptt_jmax_rows(int access_bytes) {
   return access_bytes >= 16 ? 4 : (access_bytes >= 8 ? 8 : 16);

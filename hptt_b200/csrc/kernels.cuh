@@ -188,38 +188,29 @@ __device__ __forceinline__ void tile_one(const HpttProblem &P, const HpttTile &T
                                          const E *__restrict__ A, E *__restrict__ B,
                                          const unsigned char *__restrict__ tables,
                                          const Op<E, MODE, UPD> &op, E *sdata, uint32_t tile) {
-  constexpr int J = hptt_jmax_tile(sizeof(E), UPD);
+  constexpr int J = hptt_jmax_tile(sizeof(E));
   using Ent = HpttTabEnt<OffT>;
   const Ent *__restrict__ tabY = reinterpret_cast<const Ent *>(tables);
   const Ent *__restrict__ tabX = reinterpret_cast<const Ent *>(tables + T.tab2_off);
   const HpttThr th = reinterpret_cast<const HpttThr *>(tables + T.thr_off)[threadIdx.x];
   const TileOrigin o = tile_origin(P, T, tile);
-  const int LD = T.LD, W = T.W, R1 = T.R1, R2 = T.R2;
+  const int LD = T.LD, W = T.W, R1 = T.R1, R2 = T.R2, J1 = T.J1, J2 = T.J2;
   const int TX = T.TX, TY = T.TY;
-  // iterations with a row (column) slot inside the tile -- and, on a
-  // single-dim side, inside the tensor
-  int nL = (th.cxe < o.remX) ? th.nld : 0;
-  int nS = (th.cye2 < o.remY) ? th.nst : 0;
-  if (LY && T.yc >= 0 && o.remY < TY)
-    nL = min(nL, valid_iters(o.remY, th.q0, T.r1_mul, T.r1_shr, R1));
-  if (LX && T.xc >= 0 && o.remX < TX)
-    nS = min(nS, valid_iters(o.remX, th.qs0, T.r2_mul, T.r2_shr, R2));
-  // single-dim sides: in-tile offsets fit 32 bits (OffT is 32-bit there)
+  const bool ld_ok = (th.active & 1) && th.cxe < o.remX;
+  const bool st_ok = (th.active & 2) && th.cye2 < o.remY;
   const int sY = (LY && T.ny == 1) ? static_cast<int>(P.sA[T.yd[0]]) : 0;
   const int sX = (LX && T.nx == 1) ? static_cast<int>(P.sB[T.xd[0]]) : 0;
-
-  // Loads never branch on table contents: an out-of-range row or column
-  // re-reads the tile's own first element (always inside: its coordinates
-  // along the chunked dims are 0), so all loads issue back to back.
+  const int limQY = (LY && T.yc >= 0 && o.remY < TY) ? o.remY : TY;
+  const int limQX = (LX && T.xc >= 0 && o.remX < TX) ? o.remX : TX;
   E v[J];
-  const E *src = A + o.bA + th.inE;
+  if (ld_ok) {
+    const E *src = A + o.bA + th.inE;
 #pragma unroll
-  for (int j = 0; j < J; ++j) {
-    if (j < nL) {
+    for (int j = 0; j < J; ++j) {
       const int q = th.q0 + j * R1;
       if (LY) {
-        v[j] = __ldg(src + q * sY);
-      } else {
+        if (j < J1 && q < limQY) v[j] = __ldg(src + q * sY);
+      } else if (j < J1 && q < TY) {
         const Ent en = tabY[q];
         v[j] = __ldg(src + (en.c < o.remY ? en.off : OffT(0)));
       }
@@ -227,46 +218,48 @@ __device__ __forceinline__ void tile_one(const HpttProblem &P, const HpttTile &T
   }
   E *dst = B + o.bB + th.outE2;
   E bv[J];
-  if (UPD) {
+  if (UPD && st_ok) {
 #pragma unroll
     for (int j = 0; j < J; ++j) {
-      if (j < nS) {
-        const int q = th.qs0 + j * R2;
-        if (LX) {
-          bv[j] = dst[q * sX];
-        } else {
-          const Ent en = tabX[q];
-          bv[j] = dst[en.c < o.remX ? en.off : OffT(0)];
-        }
+      const int q = th.qs0 + j * R2;
+      if (LX) {
+        if (j < J2 && q < limQX) bv[j] = dst[q * sX];
+      } else if (j < J2 && q < TX) {
+        const Ent en = tabX[q];
+        bv[j] = dst[en.c < o.remX ? en.off : OffT(0)];
       }
     }
   }
-  {
+  if (ld_ok) {
     E *s = sdata + th.q0 * LD + th.sme;
 #pragma unroll
-    for (int j = 0; j < J; ++j)
-      if (j < nL) s[j * R1 * LD] = v[j];
+    for (int j = 0; j < J; ++j) {
+      const int q = th.q0 + j * R1;
+      if (j < J1 && q < (LY ? limQY : TY)) s[j * R1 * LD] = v[j];
+    }
   }
   __syncthreads();
+  if (!st_ok) return;
   const E *s = sdata + th.sme2 + th.qs0 * W;
 #pragma unroll
   for (int j = 0; j < J; ++j) {
-    if (j < nS) {
-      const int q = th.qs0 + j * R2;
-      bool ok = true;
-      int64_t off;
-      if (LX) {
-        off = q * sX;
-      } else {
-        const Ent en = tabX[q];
-        ok = en.c < o.remX;
-        off = static_cast<int64_t>(en.off);
-      }
-      if (ok) {
-        const E a = s[j * R2 * W];
-        const E r = op(a, UPD ? bv[j] : a);
-        if (UPD) dst[off] = r; else __stcs(dst + off, r);
-      }
+    const int q = th.qs0 + j * R2;
+    bool ok;
+    int64_t off;
+    if (LX) {
+      ok = j < J2 && q < limQX;
+      off = q * sX;
+    } else {
+      ok = j < J2 && q < TX;
+      Ent en{};
+      if (ok) en = tabX[q];
+      ok = ok && en.c < o.remX;
+      off = static_cast<int64_t>(en.off);
+    }
+    if (ok) {
+      const E a = s[j * R2 * W];
+      const E r = op(a, UPD ? bv[j] : a);
+      if (UPD) dst[off] = r; else __stcs(dst + off, r);
     }
   }
 }

@@ -261,12 +261,6 @@ HpttThr tile_thread_consts(const HpttProblem &p, const HpttTile &t, const TileMa
               static_cast<int64_t>(w) * p.sB[0];
     h.sme2 = m.qrow[y] * t.LD + w;
   }
-  auto count = [](int lim, int q0, int R, int J) {
-    if (q0 >= lim) return 0;
-    return std::min(J, (lim - q0 + R - 1) / R);
-  };
-  h.nld = static_cast<int16_t>(ld ? count(t.TY, h.q0, t.R1, t.J1) : 0);
-  h.nst = static_cast<int16_t>(st ? count(t.TX, h.qs0, t.R2, t.J2) : 0);
   return h;
 }
 
@@ -341,8 +335,9 @@ struct Side {
 };
 
 bool shape_ok(const TileParams &tp, int64_t W, const Side &X, const Side &Y,
-              int sz, int update) {
-  const int kJMax = hptt_jmax_tile(sz, update);
+              int sz) {
+  const int kJMax = tp.max_iters > 0 ? std::min(tp.max_iters, hptt_jmax_tile(sz))
+                                     : hptt_jmax_tile(sz);
   const int64_t TX = X.prod(), TY = Y.prod();
   const int64_t RW = W * TX, WTY = W * TY;
   if (RW > tp.nt || WTY > tp.nt) return false;
@@ -475,6 +470,7 @@ int choose_rows(const HpttProblem &p, const TileParams &tp, HpttTile *t) {
 }  // namespace
 
 int choose_tile(const HpttProblem &p, const TileParams &tp, int update, HpttTile *t) {
+  (void)update;  // the shapes are the same with and without the B read
   const int sz = elem_bytes(p.dtype);
   const int r = p.rank;
   const bool common = p.perm[0] == 0;
@@ -537,7 +533,7 @@ int choose_tile(const HpttProblem &p, const TileParams &tp, int update, HpttTile
     pick_y();
   }
   // shrink until the shape fits the thread mapping (the larger side first)
-  for (int guard = 0; guard < 4096 && !shape_ok(tp, W, X, Y, sz, update); ++guard) {
+  for (int guard = 0; guard < 4096 && !shape_ok(tp, W, X, Y, sz); ++guard) {
     Side *S = (X.prod() >= Y.prod()) ? &X : &Y;
     if (S->d.empty()) S = (S == &X) ? &Y : &X;
     if (S->d.empty()) break;
@@ -583,7 +579,7 @@ int choose_tile(const HpttProblem &p, const TileParams &tp, int update, HpttTile
         const int64_t old = tt;
         const int64_t want = std::min<int64_t>(p.n[d], std::max<int64_t>(old + 1, old * 2));
         tt = want;
-        while (tt > old && !shape_ok(tp, W, X, Y, sz, update)) --tt;
+        while (tt > old && !shape_ok(tp, W, X, Y, sz)) --tt;
         if (tt > old) grown = true; else tt = old;
       } else {
         if (!S.d.empty() && S.t.back() < p.n[S.d.back()]) continue;
@@ -595,8 +591,8 @@ int choose_tile(const HpttProblem &p, const TileParams &tp, int update, HpttTile
         int64_t &tt = S.t.back();
         const int64_t want = std::min<int64_t>(p.n[d], cdiv(vmin, vol()));
         tt = std::max<int64_t>(1, want);
-        while (tt > 1 && !shape_ok(tp, W, X, Y, sz, update)) --tt;
-        if (tt > 1 && shape_ok(tp, W, X, Y, sz, update)) {
+        while (tt > 1 && !shape_ok(tp, W, X, Y, sz)) --tt;
+        if (tt > 1 && shape_ok(tp, W, X, Y, sz)) {
           grown = true;
         } else {
           S.d.pop_back();
@@ -618,12 +614,12 @@ int choose_tile(const HpttProblem &p, const TileParams &tp, int update, HpttTile
     const int64_t old = tt;
     if (2 * n <= 3 * tt) {
       tt = n;
-      if (shape_ok(tp, W, X, Y, sz, update)) continue;
+      if (shape_ok(tp, W, X, Y, sz)) continue;
       tt = old;
     }
     tt = cdiv(n, cdiv(n, old));
   }
-  if (!shape_ok(tp, W, X, Y, sz, update)) return ST_TOO_LARGE;
+  if (!shape_ok(tp, W, X, Y, sz)) return ST_TOO_LARGE;
 
   t->W = static_cast<int32_t>(W);
   t->nx = static_cast<int32_t>(X.d.size());

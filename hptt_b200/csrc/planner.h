@@ -40,6 +40,8 @@ struct TileParams {
   int ctas_per_sm = 0;     // 0: as many as fit
   int max_vec_bytes = 16;  // widest vector access (KIND_ROWS)
   int y_first = 0;         // choose the output-side dims before the input side
+  int max_iters = 0;       // cap on per-thread iterations of a tile (0: the
+                           // kernel's own limit, hptt_jmax_tile)
 };
 
 // Reference argument guard (src/hptt.cc:25-56) plus the one check the

@@ -59,7 +59,8 @@ int replay_tile(const HpttProblem &P, const HpttTile &T, int update, const Layou
                 const std::vector<unsigned char> &tab, std::vector<uint8_t> &writes,
                 uint64_t *checked) {
   const int esz = elem_bytes(P.dtype);
-  const int J = hptt_jmax_tile(esz, update);
+  const int J = hptt_jmax_tile(esz);
+  (void)update;
   if (T.J1 > J || T.J2 > J) return 101;
   if (T.smem_bytes < T.TY * T.LD * esz) return 102;
   using Ent = HpttTabEnt<OffT>;
@@ -89,20 +90,25 @@ int replay_tile(const HpttProblem &P, const HpttTile &T, int update, const Layou
   std::vector<int64_t> slot(smem_elems);
   // the kernel's single-dim-side variants (kernels.cu: pick_tile)
   const bool ly = !T.big_offsets && T.ny <= 1, lx = !T.big_offsets && T.nx <= 1;
+  // the kernel indexes single-dim sides as q * stride in 32-bit ints
+  if (ly && T.ny == 1 && T.TY > 1 && P.sA[T.yd[0]] > 0x7fffffffLL) return 128;
+  if (lx && T.nx == 1 && T.TX > 1 && P.sB[T.xd[0]] > 0x7fffffffLL) return 129;
   for (uint32_t tile = 0; tile < T.num_tiles; ++tile) {
     const TileOrigin o = tile_origin(P, T, tile);
     std::fill(slot.begin(), slot.end(), -1);
-    // load phase, with the kernel's iteration counts
+    const int limQY = (ly && T.yc >= 0 && o.remY < T.TY) ? o.remY : T.TY;
+    const int limQX = (lx && T.xc >= 0 && o.remX < T.TX) ? o.remX : T.TX;
+    // load phase: iteration j of a thread loads row slot q0 + j*R1 when
+    // j < J1 and the slot is inside the tile (single-dim Y side: inside the
+    // tensor too); a table slot outside the tensor re-reads element 0
     for (int t = 0; t < T.nt; ++t) {
       const HpttThr &th = thr[t];
-      int nL = (th.cxe < o.remX) ? th.nld : 0;
-      if (ly && T.yc >= 0 && o.remY < T.TY)
-        nL = std::min(nL, valid_iters(o.remY, th.q0, T.r1_mul, T.r1_shr, T.R1));
-      if (nL > 0 && !(th.active & 1)) return 124;
+      const bool ld_ok = (th.active & 1) && th.cxe < o.remX;
+      if (!ld_ok) continue;
       for (int j = 0; j < J; ++j) {
-        if (!(j < nL)) continue;
         const int q = th.q0 + j * T.R1;
-        if (!(j < T.J1 && q < T.TY)) return 125;
+        if (!(j < T.J1 && q < (ly ? limQY : T.TY))) continue;
+        if (q < 0 || q >= T.TY) return 125;
         if (ly && !(tabY[q].c < o.remY)) return 121;
         const int64_t si = static_cast<int64_t>(q) * T.LD + th.sme;
         if (si < 0 || si >= smem_elems) return 108;
@@ -122,14 +128,12 @@ int replay_tile(const HpttProblem &P, const HpttTile &T, int update, const Layou
     // store phase (and the B reads of the load phase, same addresses)
     for (int t = 0; t < T.nt; ++t) {
       const HpttThr &th = thr[t];
-      int nS = (th.cye2 < o.remY) ? th.nst : 0;
-      if (lx && T.xc >= 0 && o.remX < T.TX)
-        nS = std::min(nS, valid_iters(o.remX, th.qs0, T.r2_mul, T.r2_shr, T.R2));
-      if (nS > 0 && !(th.active & 2)) return 126;
+      const bool st_ok = (th.active & 2) && th.cye2 < o.remY;
+      if (!st_ok) continue;
       for (int j = 0; j < J; ++j) {
-        if (!(j < nS)) continue;
         const int q = th.qs0 + j * T.R2;
-        if (!(j < T.J2 && q < T.TX)) return 127;
+        if (!(j < T.J2 && q < (lx ? limQX : T.TX))) continue;
+        if (q < 0 || q >= T.TX) return 127;
         if (lx && !(tabX[q].c < o.remX)) return 122;
         if (!(tabX[q].c < o.remX)) {
           // the B prefetch re-reads this thread's first store element
@@ -233,10 +237,11 @@ extern "C" int hptt_cuda_debug_check_indexing(int dtype, uint32_t rank, const ui
   }
   L.nB = s;
   // both tile strategies (input side first / output side first), both
-  // update settings
-  for (int variant = 0; variant < 4; ++variant) {
+  // update settings, both per-thread iteration limits the tuner tries
+  for (int variant = 0; variant < 8; ++variant) {
     const int update = variant & 1;
-    tp.y_first = variant >> 1;
+    tp.y_first = (variant >> 1) & 1;
+    tp.max_iters = (variant >> 2) ? hptt_jmax_tile(elem_bytes(P.dtype)) / 2 : 0;
     HpttTile T;
     st = choose_tile(P, tp, update, &T);
     if (st != ST_OK) return st;
