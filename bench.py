@@ -2,7 +2,8 @@
 """Benchmark: B = alpha * A(perm) + beta * B on B200.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload sweep|plain|hard]
+                    [--workload sweep|plain|hard] [--tune-cache PATH | --no-tune-cache]
+                    [--case I]
 
 Default workload ("sweep"): the plain permutation sweep -- 48 seeded cases over
 ranks 2-6 in f32/f64, random non-identity permutations, extents log-uniform in
@@ -16,7 +17,11 @@ e2e       = the same metric through the C ABI with host buffers: every step
             copies A (and B when it is read) from pinned host memory, runs
             exec, and copies B back, all inside the timed region
 roofline  = the dominant kernel's achieved bandwidth over the measured HBM
-            copy peak (MEASURED_PEAKS.json)
+            copy peak (MEASURED_PEAKS.json); traffic = its DRAM bytes per
+            launch from the committed ncu summary (profiles/traffic.json)
+tiles     = from the shipped autotune cache (hptt_b200/tune/b200.cache, made
+            on a B200 by `python -m hptt_b200.tune_sweep`); a shape it does
+            not hold uses the planner's heuristic (--no-tune-cache: always)
 cpu_baseline = the reference's own CPU plan (oracle/_ref, built from the
             reference sources) on a bounded sample of the same workload, all
             host threads; shapes where the reference plan is incorrect are
@@ -43,6 +48,7 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "GB/s & % HBM peak per transpose; batched req/s + p99 vs plain per-call exec"
+DEFAULT_TUNE_CACHE = os.path.join(ROOT, "hptt_b200", "tune", "b200.cache")
 
 
 def _peaks():
@@ -138,7 +144,15 @@ def run_ours(args, rank, world, dist):
     dev = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(dev)
     cases, desc = _workload(args.workload)
+    if args.case is not None:
+        cases = [cases[args.case]]
+        desc += f" -- transpose {args.case} only"
     stream = torch.cuda.current_stream()
+    tiles = "planner heuristic"
+    if not args.no_tune_cache and args.tune_cache and os.path.exists(args.tune_cache):
+        h.tune_cache_load(args.tune_cache)
+        tiles = (f"autotune cache {os.path.relpath(args.tune_cache, ROOT)} "
+                 f"({h.tune_cache_size()} entries; heuristic on a miss)")
 
     # resident buffers: one A and one B per distinct tensor shape
     bufs = {}
@@ -217,12 +231,14 @@ def run_ours(args, rank, world, dist):
     dom_ms, dom_bytes, dom_launches = by_kind[dom]
     peak, peak_kind = _peaks()
     achieved = dom_bytes / (dom_ms / 1e3) / 1e9
-    traffic = _profiled_traffic(dom)
+    # the committed launch list covers the full sweep step
+    traffic = _profiled_traffic(dom) if args.workload == "sweep" and args.case is None else None
     roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak,
                 "unit": "GB/s", "frac": round(achieved / peak, 4),
                 "traffic": traffic, "kernel": "k_tile" if dom == "tile" else "k_rows",
                 "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs, burst copy)",
                 "launches": dom_launches,
+                "algorithmic_bytes_per_launch": int(dom_bytes // max(1, dom_launches)),
                 "share_of_device_time": round(dom_ms / device_ms, 4)}
 
     e2e = run_e2e(args, plans, bufs, stream) if args.e2e_steps > 0 else None
@@ -240,6 +256,7 @@ def run_ours(args, rank, world, dist):
         "data": "synthetic (seeded uniform[-1,1]; shapes from the workload generator)",
         "config": {"workload": desc, "transposes_per_step": len(plans),
                    "bytes_per_step": bytes_step, "l2": "inputs larger than L2 (no flush)",
+                   "tiles": tiles,
                    "parallelism": f"replicas x{world}"},
         "hbm_frac": round(value / world / peak, 4),
         "roofline": roofline,
@@ -253,14 +270,15 @@ def run_ours(args, rank, world, dist):
 
 
 def _profiled_traffic(kind):
-    """DRAM bytes per launch of the dominant kernel from the committed ncu
-    summary (profiles/*.json), when one exists."""
+    """DRAM bytes (read + write) per launch of the dominant kernel, averaged
+    over its launches in one step of the sweep, from the committed ncu launch
+    list (profiles/traffic.json; see profiles/k_tile_sweep_launches.md)."""
     p = os.path.join(ROOT, "profiles", "traffic.json")
     if not os.path.exists(p):
         return None
     try:
-        d = json.load(open(p))
-        return d.get(kind)
+        d = json.load(open(p)).get(kind)
+        return int(d["dram_bytes_per_launch"]) if d else None
     except Exception:
         return None
 
@@ -430,7 +448,7 @@ def run_reference(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=60)
+    ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="sweep", choices=["sweep", "plain", "hard"])
@@ -438,6 +456,13 @@ def main():
     ap.add_argument("--cpu-budget", type=float, default=20.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--ref-cases-per-step", type=int, default=4)
+    ap.add_argument("--tune-cache", default=DEFAULT_TUNE_CACHE,
+                    help="autotune cache to load before planning (tiles tuned offline on "
+                         "this GPU model by `python -m hptt_b200.tune_sweep`)")
+    ap.add_argument("--no-tune-cache", action="store_true",
+                    help="plan with the heuristic only")
+    ap.add_argument("--case", type=int, default=None,
+                    help="run only transpose I of the workload (profiling)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 

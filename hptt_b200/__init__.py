@@ -91,6 +91,10 @@ def load_library() -> ctypes.CDLL:
         "hptt_cuda_plan_destroy": (c_int, [c_vp]),
         "hptt_cuda_plan_inspect": (c_int, [c_int, c_u32, _u32p, _u32p, _u32p, _u32p,
                                            ctypes.c_char_p, c_sz]),
+        "hptt_cuda_tune_cache_load": (c_int, [ctypes.c_char_p]),
+        "hptt_cuda_tune_cache_save": (c_int, [ctypes.c_char_p]),
+        "hptt_cuda_tune_cache_clear": (c_int, []),
+        "hptt_cuda_tune_cache_size": (c_int, [ctypes.POINTER(c_u32)]),
         "hptt_cuda_status_string": (ctypes.c_char_p, [c_int]),
         "hptt_cuda_version": (ctypes.c_char_p, []),
     }
@@ -286,6 +290,31 @@ def inspect_plan(dtype, in_size: Sequence[int], perm: Sequence[int],
     if st != 0:
         raise HpttError(st, "inspect_plan")
     return buf.value.decode()
+
+
+def tune_cache_load(path: Optional[str] = None) -> None:
+    """Merge the autotune entries of a cache file (None: the file named by
+    HPTT_B200_TUNE_CACHE)."""
+    st = load_library().hptt_cuda_tune_cache_load(path.encode() if path else None)
+    if st != 0:
+        raise HpttError(st, f"tune_cache_load({path})")
+
+
+def tune_cache_save(path: Optional[str] = None) -> None:
+    """Write every autotune entry to `path` (None: HPTT_B200_TUNE_CACHE)."""
+    st = load_library().hptt_cuda_tune_cache_save(path.encode() if path else None)
+    if st != 0:
+        raise HpttError(st, f"tune_cache_save({path})")
+
+
+def tune_cache_clear() -> None:
+    load_library().hptt_cuda_tune_cache_clear()
+
+
+def tune_cache_size() -> int:
+    n = ctypes.c_uint32(0)
+    load_library().hptt_cuda_tune_cache_size(ctypes.byref(n))
+    return int(n.value)
 
 
 def version() -> str:

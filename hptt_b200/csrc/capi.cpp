@@ -319,6 +319,21 @@ int hptt_cuda_plan_inspect(int dtype, uint32_t rank, const uint32_t *in_size,
   return HPTT_OK;
 }
 
+int hptt_cuda_tune_cache_load(const char *path) { return autotune_cache_load(path); }
+
+int hptt_cuda_tune_cache_save(const char *path) { return autotune_cache_save(path); }
+
+int hptt_cuda_tune_cache_clear(void) {
+  autotune_cache_clear();
+  return HPTT_OK;
+}
+
+int hptt_cuda_tune_cache_size(uint32_t *count) {
+  if (!count) return HPTT_ERR_HANDLE;
+  *count = static_cast<uint32_t>(autotune_cache_size());
+  return HPTT_OK;
+}
+
 const char *hptt_cuda_status_string(int status) { return status_string(status); }
 
 const char *hptt_cuda_version(void) { return "hptt-b200 0.1 (sm_100a)"; }

@@ -200,6 +200,23 @@ int hptt_cuda_transpose_noalloc(int dtype, uint32_t rank, const uint32_t *in_siz
  * the reference. */
 size_t hptt_cuda_noalloc_table_bytes(void);
 
+/* Autotune cache: the tile parameters the tuner picked, one entry per
+ * (GPU name, dtype, fused rank, fused perm, size class, B read).  Plans
+ * created with tuning_timeout == 0 use a matching entry instead of the
+ * heuristic.  The file named by the environment variable
+ * HPTT_B200_TUNE_CACHE is read on first use and rewritten after every tuning
+ * run.  Replaces the reference's in-plan tuning state, which lives only as
+ * long as the plan (inc/hptt/plan/plan_trans.tcc:33-67); no reference
+ * counterpart for persistence.
+ *   load   merge the entries of a cache file (NULL: re-read the variable's)
+ *   save   write every entry (NULL: to the variable's file; no-op if unset)
+ *   clear  drop every entry (the variable's file is not read again)
+ *   size   number of entries in *count */
+int hptt_cuda_tune_cache_load(const char *path);
+int hptt_cuda_tune_cache_save(const char *path);
+int hptt_cuda_tune_cache_clear(void);
+int hptt_cuda_tune_cache_size(uint32_t *count);
+
 /* Static text for a status code. */
 const char *hptt_cuda_status_string(int status);
 
