@@ -27,6 +27,15 @@ cpu_baseline = the reference's own CPU plan (oracle/_ref, built from the
             host threads; shapes where the reference plan is incorrect are
             timed with the reference's naive RefTrans instead, labelled.
 
+served   = the served form: Poisson arrivals over the same 4096 plans at
+            10k-500k requests/s (2 s windows by default, --serve-seconds 60
+            for the full run), 32 GB admission budget, continuous batching vs
+            the plain per-call loop: throughput and p50/p99/p99.9 latency
+            (--no-served skips it)
+batched  = the batched form on the 4096-transpose mixed workload: one graph
+            launch per run vs one plain exec per transpose (C loop, and the
+            Python loop), same plans and buffers (--no-batched skips it)
+
 N > 1 (torchrun): every rank runs the whole workload on its own GPU
 (independent transposes; no collective on the data path), scaling "weak".
 `--impl reference` times only the reference's CPU implementation (rank 0).
@@ -131,6 +140,23 @@ class ClockSampler:
 # --------------------------------------------------------------------------
 # our arm
 # --------------------------------------------------------------------------
+def max_over_ranks(x: float, dist, world: int, device: str = "cuda") -> float:
+    """The largest of every rank's x (x itself on one rank).  Every rank must
+    call it at the same point: it is one all-reduce."""
+    if world <= 1 or dist is None:
+        return float(x)
+    import torch
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t[0])
+
+
+def aggregate_gbs(bytes_per_rank: int, world: int, max_ms: float) -> float:
+    """Whole-job throughput: the bytes all ranks moved over the slowest rank's
+    time (every rank runs the same workload: replicas, weak scaling)."""
+    return bytes_per_rank * world / (max_ms / 1e3) / 1e9
+
+
 def _tdtype(torch, name):
     return {"f32": torch.float32, "f64": torch.float64, "c64": torch.complex64,
             "c128": torch.complex128}[name]
@@ -209,15 +235,11 @@ def run_ours(args, rank, world, dist):
     elapsed_ms = t0.elapsed_time(t1)
     per_launch_ms = [sum(ev[k][i][0].elapsed_time(ev[k][i][1]) for k in range(args.steps))
                      for i in range(len(plans))]
-    if world > 1:
-        tt = torch.tensor([elapsed_ms], device="cuda", dtype=torch.float64)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        elapsed_ms = float(tt[0])
+    elapsed_ms = max_over_ranks(elapsed_ms, dist, world)
     device_ms = sum(per_launch_ms)
 
     bytes_step = sum(bb for _, bb, _, _ in plans)
-    total_bytes = bytes_step * args.steps * world
-    value = total_bytes / (elapsed_ms / 1e3) / 1e9
+    value = aggregate_gbs(bytes_step * args.steps, world, elapsed_ms)
     ms_per_step = elapsed_ms / args.steps
 
     # dominant kernel: the kernel kind with the most device time
@@ -241,7 +263,17 @@ def run_ours(args, rank, world, dist):
                 "algorithmic_bytes_per_launch": int(dom_bytes // max(1, dom_launches)),
                 "share_of_device_time": round(dom_ms / device_ms, 4)}
 
-    e2e = run_e2e(args, plans, bufs, stream) if args.e2e_steps > 0 else None
+    e2e = run_e2e(args, plans, bufs, stream, dist, world) if args.e2e_steps > 0 else None
+    # the batched and served forms are measured on one GPU (N > 1 runs
+    # replicas of the sweep only)
+    batched = served = None
+    if world == 1 and args.case is None and not (args.no_batched and args.no_served):
+        pool, pool_buffers = _batch_pool(args)
+        if not args.no_batched:
+            batched = run_batched(args, stream, pool)
+        if not args.no_served:
+            served = run_served(args, pool)
+        del pool, pool_buffers
     gpu_launches = sum(p.launches for p, _, _, _ in plans) * args.steps
 
     cpu = None
@@ -264,6 +296,8 @@ def run_ours(args, rank, world, dist):
         "gpu_launches": gpu_launches,
         "clocks": clocks,
         "cpu_baseline": cpu,
+        "batched": batched,
+        "served": served,
         "kernel_ms_per_step": round(device_ms / args.steps, 4),
     }
     return out
@@ -283,53 +317,199 @@ def _profiled_traffic(kind):
         return None
 
 
-def run_e2e(args, plans, bufs, stream):
-    """Same workload through the C ABI with host buffers, copies timed."""
+def run_e2e(args, plans, bufs, stream, dist=None, world=1):
+    """Same workload through the C ABI with host buffers, copies timed.
+
+    Every transpose copies its A (and B when B is read) from pinned host
+    memory into a device staging pair, points its plan there (reset_data),
+    runs exec, and copies B back to pinned host memory.  Transposes alternate
+    between two streams with one staging pair each, so one transpose's
+    host->device copy overlaps the previous one's device->host copy (PCIe is
+    full duplex) and the kernel in between."""
     import torch
-    # pinned host staging, one set per distinct tensor size (reused)
     host = {}
     for key, (a, b) in bufs.items():
-        host[key] = (torch.empty_like(a, device="cpu").pin_memory(),
-                     torch.empty_like(b, device="cpu").pin_memory(),
-                     torch.empty_like(b, device="cpu").pin_memory())
-        host[key][0].copy_(a.cpu())
-        host[key][1].copy_(b.cpu())
+        ha = torch.empty_like(a, device="cpu").pin_memory()
+        hb = torch.empty_like(b, device="cpu").pin_memory()
+        ha.copy_(a.cpu())
+        hb.copy_(b.cpu())
+        host[key] = (ha, hb)
+    max_bytes = max(a.numel() * a.element_size() for a, _ in bufs.values())
+    streams = [torch.cuda.Stream(), torch.cuda.Stream()]
+    stage = [(torch.empty(max_bytes, dtype=torch.uint8, device="cuda"),
+              torch.empty(max_bytes, dtype=torch.uint8, device="cuda"),
+              torch.empty(max_bytes, dtype=torch.uint8).pin_memory()) for _ in streams]
     h2d = d2h = 0
-    keys = []
+    work = []
     for p, bb, kind, c in plans:
         key = (c["dtype"], tuple(c["in_size"]), tuple(c["perm"]))
-        keys.append(key)
-        nbytes = bufs[key][0].numel() * bufs[key][0].element_size()
+        a, _ = bufs[key]
+        nbytes = a.numel() * a.element_size()
         reads_b = bb > 2 * nbytes
         h2d += nbytes * (2 if reads_b else 1)
         d2h += nbytes
+        work.append((p, key, nbytes, reads_b, a.dtype))
 
     def step():
-        for (p, bb, kind, c), key in zip(plans, keys):
-            a, b = bufs[key]
-            ha, hb, hout = host[key]
-            a.copy_(ha, non_blocking=True)
-            if bb > 2 * a.numel() * a.element_size():
-                b.copy_(hb, non_blocking=True)
-            p.exec_on(stream.cuda_stream)
-            hout.copy_(b, non_blocking=True)
+        for i, (p, key, nbytes, reads_b, dt) in enumerate(work):
+            s = streams[i % 2]
+            sa, sb, hout = stage[i % 2]
+            ha, hb = host[key]
+            da = sa[:nbytes].view(dt)
+            db = sb[:nbytes].view(dt)
+            with torch.cuda.stream(s):
+                da.copy_(ha, non_blocking=True)
+                if reads_b:
+                    db.copy_(hb, non_blocking=True)
+                p.reset_data(da, db)
+                p.exec_on(s.cuda_stream)
+                hout[:nbytes].view(dt).copy_(db, non_blocking=True)
 
-    for _ in range(min(1, args.warmup)):
-        step()
-    torch.cuda.synchronize()
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    for _ in range(args.e2e_steps):
-        step()
-    e1.record(stream)
-    torch.cuda.synchronize()
-    ms = e0.elapsed_time(e1)
+    def timed(nsteps):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for s in streams:
+            s.wait_event(e0)
+        for _ in range(nsteps):
+            step()
+        for s in streams:
+            ev = torch.cuda.Event()
+            ev.record(s)
+            stream.wait_event(ev)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1)
+
+    timed(1)  # warm-up
+    ms = timed(args.e2e_steps)
+    ms = max_over_ranks(ms, dist, world)
     total = sum(bb for _, bb, _, _ in plans) * args.e2e_steps
-    return {"value": round(total / (ms / 1e3) / 1e9, 2), "unit": "GB/s",
-            "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+    return {"value": round(aggregate_gbs(total, world, ms), 2), "unit": "GB/s",
+            "h2d_bytes_per_step": h2d * world, "d2h_bytes_per_step": d2h * world,
             "steps": args.e2e_steps, "ms_per_step": round(ms / args.e2e_steps, 3),
-            "api": "hptt_cuda_plan_exec_on (C ABI) + pinned host<->device copies"}
+            "api": "TransPlan.reset_data + exec_on (C ABI) with pinned host<->device "
+                   "copies, two streams"}
+
+
+def _batch_pool(args):
+    """The mixed workload's plans and resident buffers: 4096 transposes
+    (f32/f64/c64/c128, ranks 2-6, 4 KB - 16 MB per tensor, half alpha=1/
+    beta=0, complex scalars for complex types), tiles from the autotune
+    cache.  16.6 GB of tensors, far larger than L2 (no flush needed)."""
+    import torch
+    import hptt_b200 as h
+    from hptt_b200 import workloads as w
+
+    cases = w.batch_cases(count=args.batch_count)
+    g = torch.Generator(device="cuda").manual_seed(77)
+    plans, keep = [], []
+    for c in cases:
+        n = int(np.prod(c["in_size"]))
+        t = _tdtype(torch, c["dtype"])
+        if c["dtype"] in ("c64", "c128"):
+            rt = torch.float32 if c["dtype"] == "c64" else torch.float64
+            a = torch.view_as_complex(torch.rand(n, 2, generator=g, device="cuda", dtype=rt) * 2 - 1)
+            b = torch.view_as_complex(torch.rand(n, 2, generator=g, device="cuda", dtype=rt) * 2 - 1)
+        else:
+            a = torch.rand(n, generator=g, device="cuda", dtype=t) * 2 - 1
+            b = torch.rand(n, generator=g, device="cuda", dtype=t) * 2 - 1
+        p = h.create_plan(a, b, c["in_size"], c["perm"], c["alpha"], c["beta"], 0,
+                          dtype=c["dtype"])
+        assert p is not None
+        plans.append(p)
+        keep.append((a, b))
+    return plans, keep
+
+
+def run_batched(args, stream, plans):
+    """The batched form on the mixed workload pool.  One run = the whole
+    set, timed three ways on the same plans and buffers:
+      batch     one graph launch (hptt_cuda_batch_exec)
+      per_call  one plain exec per transpose from a C loop
+                (hptt_cuda_plan_exec_many)
+      per_call_python  one TransPlan.exec_on per transpose from Python"""
+    import torch
+    import hptt_b200 as h
+
+    batch = h.create_batch(plans)
+    nbytes, items, kernels = batch.info()
+    sptr = stream.cuda_stream
+
+    def timed(fn, reps):
+        fn()
+        fn()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(reps):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+    reps = max(3, args.batch_reps)
+    batch_ms = timed(lambda: batch.exec(sptr), reps)
+    call_ms = timed(lambda: h.exec_many(plans, sptr), reps)
+
+    def py_loop():
+        for p in plans:
+            p.exec_on(sptr)
+    py_ms = timed(py_loop, 3)
+    n = len(plans)
+    out = {
+        "workload": f"{n} mixed transposes (f32/f64/c64/c128, ranks 2-6, 4 KB-16 MB per "
+                    "tensor, half alpha=1/beta=0, complex scalars for complex types)",
+        "transposes": n,
+        "bytes_per_run": nbytes, "work_items": items, "kernels_per_run": kernels,
+        "batch": {"ms": round(batch_ms, 4), "GB/s": round(nbytes / batch_ms / 1e6, 1),
+                  "transposes_per_s": round(n / batch_ms * 1e3, 1), "launches": 1,
+                  "api": "hptt_cuda_batch_exec (one CUDA graph launch)"},
+        "per_call": {"ms": round(call_ms, 4), "GB/s": round(nbytes / call_ms / 1e6, 1),
+                     "transposes_per_s": round(n / call_ms * 1e3, 1), "launches": n,
+                     "api": "hptt_cuda_plan_exec_many (C loop of plain execs)"},
+        "per_call_python": {"ms": round(py_ms, 4), "GB/s": round(nbytes / py_ms / 1e6, 1),
+                            "api": "TransPlan.exec_on per transpose from Python"},
+        "speedup_vs_per_call": round(call_ms / batch_ms, 3),
+        "speedup_vs_per_call_python": round(py_ms / batch_ms, 3),
+        "reps": reps,
+    }
+    batch.destroy()
+    return out
+
+
+def run_served(args, plans):
+    """The served form: open-loop Poisson arrivals over the mixed pool (each
+    request a uniformly drawn plan on its resident buffers) at each rate for
+    --serve-seconds, admission budget 32 GB; continuous batching vs the plain
+    per-call loop (one exec per request, in arrival order, one stream) on the
+    same GPU.  Arrivals come from the library's native generator
+    (hptt_cuda_server_run_poisson)."""
+    import hptt_b200 as h
+
+    budget = 32 << 30
+    rates = [float(r) for r in args.serve_rates.split(",")]
+    keys = ("submitted", "completed", "launches", "mean_batch", "throughput_rps", "gbs",
+            "lat_p50_us", "lat_p99_us", "lat_p999_us", "lat_max_us", "peak_inflight_bytes",
+            "peak_pending")
+    out = {"budget_bytes": budget, "seconds_per_rate": args.serve_seconds,
+           "pool": len(plans), "rates": []}
+    for mode in ("batched", "per_call"):
+        srv = h.TransServer(budget_bytes=budget,
+                            max_inflight_launches=4 if mode == "batched" else 1024,
+                            max_batch=1024, per_call=(mode == "per_call"))
+        for k, rate in enumerate(rates):
+            st = srv.run_poisson(plans, rate=rate, seconds=args.serve_seconds, seed=1000 + k,
+                                 drain_timeout=600.0)
+            row = next((r for r in out["rates"] if r["rate"] == rate), None)
+            if row is None:
+                row = {"rate": rate}
+                out["rates"].append(row)
+            row[mode] = {kk: (round(st[kk], 2) if isinstance(st[kk], float) else st[kk])
+                         for kk in keys}
+        srv.destroy()
+    return out
 
 
 # --------------------------------------------------------------------------
@@ -461,6 +641,15 @@ def main():
                          "this GPU model by `python -m hptt_b200.tune_sweep`)")
     ap.add_argument("--no-tune-cache", action="store_true",
                     help="plan with the heuristic only")
+    ap.add_argument("--no-batched", action="store_true",
+                    help="skip the batched-form measurement")
+    ap.add_argument("--batch-count", type=int, default=4096)
+    ap.add_argument("--no-served", action="store_true",
+                    help="skip the served-form measurement")
+    ap.add_argument("--serve-rates", default="10000,30000,100000,250000,500000")
+    ap.add_argument("--serve-seconds", type=float, default=2.0,
+                    help="arrival window per rate (60 for the full served workload)")
+    ap.add_argument("--batch-reps", type=int, default=10)
     ap.add_argument("--case", type=int, default=None,
                     help="run only transpose I of the workload (profiling)")
     args = ap.parse_args()

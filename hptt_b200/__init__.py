@@ -62,6 +62,26 @@ def library_path() -> str:
     return LIB_PATH
 
 
+class ServeConfig(ctypes.Structure):
+    """hptt_cuda_serve_config"""
+    _fields_ = [("budget_bytes", ctypes.c_uint64), ("max_inflight_launches", ctypes.c_uint32),
+                ("max_batch", ctypes.c_uint32), ("per_call", ctypes.c_int32),
+                ("reserved", ctypes.c_int32)]
+
+
+class ServeStats(ctypes.Structure):
+    """hptt_cuda_serve_stats"""
+    _fields_ = [(n, ctypes.c_uint64) for n in (
+                    "submitted", "completed", "failed", "launches", "bytes",
+                    "peak_inflight_bytes", "peak_pending")] + \
+               [(n, ctypes.c_double) for n in (
+                    "elapsed_s", "throughput_rps", "gbs", "mean_batch", "lat_mean_us",
+                    "lat_p50_us", "lat_p99_us", "lat_p999_us", "lat_max_us")]
+
+    def as_dict(self):
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
 def load_library() -> ctypes.CDLL:
     """Load libhptt_cuda.so (raises if it has not been built)."""
     global _lib
@@ -91,6 +111,24 @@ def load_library() -> ctypes.CDLL:
         "hptt_cuda_plan_destroy": (c_int, [c_vp]),
         "hptt_cuda_plan_inspect": (c_int, [c_int, c_u32, _u32p, _u32p, _u32p, _u32p,
                                            ctypes.c_char_p, c_sz]),
+        "hptt_cuda_batch_create": (c_int, [ctypes.POINTER(c_vp), c_u32, ctypes.POINTER(c_vp)]),
+        "hptt_cuda_batch_refresh": (c_int, [c_vp]),
+        "hptt_cuda_batch_exec": (c_int, [c_vp, c_vp]),
+        "hptt_cuda_batch_info": (c_int, [c_vp, ctypes.POINTER(ctypes.c_uint64),
+                                         ctypes.POINTER(c_u32), ctypes.POINTER(c_u32)]),
+        "hptt_cuda_batch_destroy": (c_int, [c_vp]),
+        "hptt_cuda_plan_exec_many": (c_int, [ctypes.POINTER(c_vp), c_u32, c_vp]),
+        "hptt_cuda_server_create": (c_int, [ctypes.POINTER(ServeConfig), ctypes.POINTER(c_vp)]),
+        "hptt_cuda_server_submit": (c_int, [c_vp, c_vp, c_vp, c_vp,
+                                            ctypes.POINTER(ctypes.c_uint64)]),
+        "hptt_cuda_server_wait": (c_int, [c_vp, ctypes.c_uint64, c_dbl]),
+        "hptt_cuda_server_drain": (c_int, [c_vp, c_dbl]),
+        "hptt_cuda_server_stats": (c_int, [c_vp, ctypes.POINTER(ServeStats)]),
+        "hptt_cuda_server_reset_stats": (c_int, [c_vp]),
+        "hptt_cuda_server_run_poisson": (c_int, [c_vp, ctypes.POINTER(c_vp), c_u32, c_dbl, c_dbl,
+                                                 ctypes.c_uint64, c_dbl,
+                                                 ctypes.POINTER(ServeStats)]),
+        "hptt_cuda_server_destroy": (c_int, [c_vp]),
         "hptt_cuda_tune_cache_load": (c_int, [ctypes.c_char_p]),
         "hptt_cuda_tune_cache_save": (c_int, [ctypes.c_char_p]),
         "hptt_cuda_tune_cache_clear": (c_int, []),
@@ -290,6 +328,147 @@ def inspect_plan(dtype, in_size: Sequence[int], perm: Sequence[int],
     if st != 0:
         raise HpttError(st, "inspect_plan")
     return buf.value.decode()
+
+
+def _handles(plans) -> ctypes.Array:
+    arr = (ctypes.c_void_p * max(1, len(plans)))()
+    for i, p in enumerate(plans):
+        arr[i] = p.handle if p is not None else None
+    return arr
+
+
+class TransBatch:
+    """Many plans run by one graph launch (hptt_cuda_batch_*).  Results are
+    bit-identical to each plan's own exec.  The plans must stay alive (the
+    batch keeps references) and must not write into one another's buffers."""
+
+    def __init__(self, plans: Sequence["TransPlan"]):
+        self._plans = list(plans)
+        h = ctypes.c_void_p(0)
+        st = load_library().hptt_cuda_batch_create(_handles(self._plans), len(self._plans),
+                                                   ctypes.byref(h))
+        if st != 0:
+            raise HpttError(st, "batch_create")
+        self._h = h.value
+
+    def exec(self, stream=None) -> None:
+        """Enqueue one run of every entry (one graph launch)."""
+        st = load_library().hptt_cuda_batch_exec(self._h, _stream_ptr(stream))
+        if st != 0:
+            raise HpttError(st, "batch_exec")
+
+    def refresh(self) -> None:
+        """Re-read the plans' pointers and scalars (after reset_data / set_coef)."""
+        st = load_library().hptt_cuda_batch_refresh(self._h)
+        if st != 0:
+            raise HpttError(st, "batch_refresh")
+
+    def info(self):
+        """(algorithmic bytes per exec, work items, kernels per exec)."""
+        b, w, k = ctypes.c_uint64(0), ctypes.c_uint32(0), ctypes.c_uint32(0)
+        st = load_library().hptt_cuda_batch_info(self._h, ctypes.byref(b), ctypes.byref(w),
+                                                 ctypes.byref(k))
+        if st != 0:
+            raise HpttError(st, "batch_info")
+        return int(b.value), int(w.value), int(k.value)
+
+    @property
+    def bytes(self) -> int:
+        return self.info()[0]
+
+    def destroy(self) -> None:
+        if getattr(self, "_h", None):
+            load_library().hptt_cuda_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.destroy()
+        except Exception:
+            pass
+
+
+def create_batch(plans: Sequence["TransPlan"]) -> TransBatch:
+    return TransBatch(plans)
+
+
+def exec_many(plans: Sequence["TransPlan"], stream=None) -> None:
+    """One plain exec per plan, in order, from a C loop (the per-call form)."""
+    st = load_library().hptt_cuda_plan_exec_many(_handles(plans), len(plans),
+                                                 _stream_ptr(stream))
+    if st != 0:
+        raise HpttError(st, "exec_many")
+
+
+class TransServer:
+    """The served form (hptt_cuda_server_*): requests are queued, admitted
+    against a device-byte budget and run with continuous batching (or one
+    plain exec each with ``per_call=True``).  Buffers passed to ``submit``
+    must stay alive until the request has finished."""
+
+    def __init__(self, budget_bytes: int = 32 << 30, max_inflight_launches: int = 4,
+                 max_batch: int = 512, per_call: bool = False):
+        cfg = ServeConfig(int(budget_bytes), int(max_inflight_launches), int(max_batch),
+                          int(bool(per_call)), 0)
+        h = ctypes.c_void_p(0)
+        st = load_library().hptt_cuda_server_create(ctypes.byref(cfg), ctypes.byref(h))
+        if st != 0:
+            raise HpttError(st, "server_create")
+        self._h = h.value
+
+    def submit(self, plan: "TransPlan", in_data=None, out_data=None) -> int:
+        t = ctypes.c_uint64(0)
+        ip = _device_ptr(in_data) if in_data is not None else None
+        op = _device_ptr(out_data) if out_data is not None else None
+        st = load_library().hptt_cuda_server_submit(self._h, plan.handle, ip, op,
+                                                    ctypes.byref(t))
+        if st != 0:
+            raise HpttError(st, "server_submit")
+        return int(t.value)
+
+    def wait(self, ticket: int, timeout: float = 60.0) -> None:
+        st = load_library().hptt_cuda_server_wait(self._h, ticket, float(timeout))
+        if st != 0:
+            raise HpttError(st, f"server_wait({ticket})")
+
+    def drain(self, timeout: float = 120.0) -> None:
+        st = load_library().hptt_cuda_server_drain(self._h, float(timeout))
+        if st != 0:
+            raise HpttError(st, "server_drain")
+
+    def stats(self) -> dict:
+        s = ServeStats()
+        st = load_library().hptt_cuda_server_stats(self._h, ctypes.byref(s))
+        if st != 0:
+            raise HpttError(st, "server_stats")
+        return s.as_dict()
+
+    def reset_stats(self) -> None:
+        st = load_library().hptt_cuda_server_reset_stats(self._h)
+        if st != 0:
+            raise HpttError(st, "server_reset_stats")
+
+    def run_poisson(self, pool: Sequence["TransPlan"], rate: float, seconds: float,
+                    seed: int = 0, drain_timeout: float = 300.0) -> dict:
+        """Open-loop Poisson arrivals over `pool` (native load generator)."""
+        s = ServeStats()
+        st = load_library().hptt_cuda_server_run_poisson(
+            self._h, _handles(pool), len(pool), float(rate), float(seconds), int(seed),
+            float(drain_timeout), ctypes.byref(s))
+        if st != 0:
+            raise HpttError(st, "server_run_poisson")
+        return s.as_dict()
+
+    def destroy(self) -> None:
+        if getattr(self, "_h", None):
+            load_library().hptt_cuda_server_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.destroy()
+        except Exception:
+            pass
 
 
 def tune_cache_load(path: Optional[str] = None) -> None:

@@ -111,20 +111,30 @@ int plan_vec_for_ptrs(const Plan *p) {
   return (a % bytes == 0 && b % bytes == 0) ? p->vec : 1;
 }
 
-int plan_enqueue(Plan *p, cudaStream_t stream) {
-  if (!p->args.A || !p->args.B) return ST_NULL_DATA;
-  const int vec = plan_vec_for_ptrs(p);
+int plan_enqueue_with(const Plan *p, const void *A, void *B, cudaStream_t stream) {
+  if (!A || !B) return ST_NULL_DATA;
+  HpttArgs a = p->args;
+  a.A = A;
+  a.B = B;
+  int vec = p->vec;
+  if (vec > 1) {
+    const uintptr_t vb = static_cast<uintptr_t>(vec) * elem_bytes(a.p.dtype);
+    if (reinterpret_cast<uintptr_t>(A) % vb || reinterpret_cast<uintptr_t>(B) % vb) vec = 1;
+  }
   cudaError_t e;
   if (vec == p->vec) {
-    p->args.tables = p->dtab;
-    e = launch_single(p->args, vec, p->grid, stream);
+    a.tables = p->dtab;
+    e = launch_single(a, vec, p->grid, stream);
   } else {
-    HpttArgs a = p->args;
     a.t = p->tile_scalar;
     a.tables = p->dtab_scalar;
     e = launch_single(a, 1, p->grid_scalar, stream);
   }
   return e == cudaSuccess ? ST_OK : ST_CUDA;
+}
+
+int plan_enqueue(Plan *p, cudaStream_t stream) {
+  return plan_enqueue_with(p, p->args.A, p->args.B, stream);
 }
 
 void plan_free_tables(Plan *p) {

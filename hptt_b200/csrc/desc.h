@@ -90,6 +90,15 @@ struct HpttTile {
   // fast division by R1 and R2 (same scheme as gmul/gshr)
   uint32_t r1_mul, r2_mul;
   int32_t r1_shr, r2_shr;
+  // KIND_TILE: 1 when TY == R1 * J1 and TX == R2 * J2, so in a tile that
+  // lies wholly inside the tensor every loading thread has exactly J1 rows
+  // and every storing thread J2 columns
+  int32_t even;
+  // fast division by TX and TY: per-thread constants of single-dim tiles
+  // with W == 1 are computed from threadIdx instead of read from the table
+  uint32_t tx_mul, ty_mul;
+  int32_t tx_shr, ty_shr;
+  int32_t pad_;
 };
 
 // One slot of a KIND_TILE offset table (OffT = uint32_t or int64_t).

@@ -160,6 +160,30 @@ HPTT_HD inline int fast_div(int n, uint32_t mul, int shr) {
   return mul ? static_cast<int>(umulhi32(static_cast<uint32_t>(n), mul) >> shr) : n;
 }
 
+// Per-thread constants of a tile with one X dim, one Y dim and W == 1, from
+// the thread index alone: load element x = tid % TX of rows q0 = tid / TX,
+// store element y = tid % TY of columns qs0 = tid / TY; both slot maps are
+// the identity, so shared memory holds (x, y) at y * LD + x.  Equal to the
+// host table's entry (tile_thread_consts); the CPU replay checks that.
+HPTT_HD inline HpttThr thread_consts_1d(const HpttProblem &P, const HpttTile &T, int tid) {
+  HpttThr h;
+  const int q0 = fast_div(tid, T.tx_mul, T.tx_shr);
+  const int x = tid - q0 * T.TX;
+  const int qs0 = fast_div(tid, T.ty_mul, T.ty_shr);
+  const int y = tid - qs0 * T.TY;
+  h.q0 = q0;
+  h.qs0 = qs0;
+  h.inE = static_cast<int64_t>(x) * P.sA[T.xd[0]];
+  h.outE2 = static_cast<int64_t>(y) * P.sB[T.yd[0]];
+  h.sme = x;
+  h.sme2 = y * T.LD;
+  h.cxe = T.xc >= 0 ? x : 0;
+  h.cye2 = T.yc >= 0 ? y : 0;
+  h.active = (tid < T.R1 * T.TX ? 1 : 0) | (tid < T.R2 * T.TY ? 2 : 0);
+  h.pad = 0;
+  return h;
+}
+
 // Iterations j >= 0 with q0 + j * R < lim (R > 0): ceil((lim - q0) / R), or 0.
 HPTT_HD inline int valid_iters(int lim, int q0, uint32_t mul, int shr, int R) {
   return lim > q0 ? fast_div(lim - q0 + R - 1, mul, shr) : 0;
@@ -192,10 +216,59 @@ __device__ __forceinline__ void tile_one(const HpttProblem &P, const HpttTile &T
   using Ent = HpttTabEnt<OffT>;
   const Ent *__restrict__ tabY = reinterpret_cast<const Ent *>(tables);
   const Ent *__restrict__ tabX = reinterpret_cast<const Ent *>(tables + T.tab2_off);
-  const HpttThr th = reinterpret_cast<const HpttThr *>(tables + T.thr_off)[threadIdx.x];
+  // single-dim sides with W == 1: constants from the thread index (no table
+  // read before the first load); else the host table's entry
+  const HpttThr th = (LX && LY && T.W == 1 && T.nx == 1 && T.ny == 1)
+                         ? thread_consts_1d(P, T, threadIdx.x)
+                         : reinterpret_cast<const HpttThr *>(tables + T.thr_off)[threadIdx.x];
   const TileOrigin o = tile_origin(P, T, tile);
   const int LD = T.LD, W = T.W, R1 = T.R1, R2 = T.R2, J1 = T.J1, J2 = T.J2;
   const int TX = T.TX, TY = T.TY;
+  if (!UPD && LX && LY && T.even && o.remX >= TX && o.remY >= TY) {
+    // Interior tile of an even shape: every loading thread has exactly J1
+    // rows and every storing thread J2 columns (TY == R1*J1, TX == R2*J2),
+    // so the accesses below -- the same as the general path's -- need no
+    // per-element bounds.  Offsets fit 32 bits (single-dim sides imply
+    // 32-bit tables, i.e. in-tile offsets below 2^31).
+    const int sYf = T.ny == 1 ? static_cast<int>(P.sA[T.yd[0]]) : 0;
+    const int sXf = T.nx == 1 ? static_cast<int>(P.sB[T.xd[0]]) : 0;
+    const bool ld = th.active & 1, st = th.active & 2;
+    E v[J];
+    const E *src = A + o.bA + th.inE + th.q0 * sYf;
+    const int stepA = R1 * sYf;
+    if (ld) {
+#pragma unroll
+      for (int j = 0; j < J; ++j)
+        if (j < J1) v[j] = __ldg(src + j * stepA);
+    }
+    E *dst = B + o.bB + th.outE2 + th.qs0 * sXf;
+    const int stepB = R2 * sXf;
+    E bv[J];
+    if (UPD && st) {
+#pragma unroll
+      for (int j = 0; j < J; ++j)
+        if (j < J2) bv[j] = dst[j * stepB];
+    }
+    if (ld) {
+      E *s = sdata + th.q0 * LD + th.sme;
+#pragma unroll
+      for (int j = 0; j < J; ++j)
+        if (j < J1) s[j * R1 * LD] = v[j];
+    }
+    __syncthreads();
+    if (st) {
+      const E *s = sdata + th.sme2 + th.qs0 * W;
+#pragma unroll
+      for (int j = 0; j < J; ++j) {
+        if (j < J2) {
+          const E a = s[j * R2 * W];
+          const E r = op(a, UPD ? bv[j] : a);
+          if (UPD) dst[j * stepB] = r; else __stcs(dst + j * stepB, r);
+        }
+      }
+    }
+    return;
+  }
   const bool ld_ok = (th.active & 1) && th.cxe < o.remX;
   const bool st_ok = (th.active & 2) && th.cye2 < o.remY;
   const int sY = (LY && T.ny == 1) ? static_cast<int>(P.sA[T.yd[0]]) : 0;

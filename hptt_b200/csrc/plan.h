@@ -42,6 +42,9 @@ int plan_tiles(Plan *p, const TileParams &params);
 // Enqueue one exec of the plan on `stream`.
 int plan_enqueue(Plan *p, cudaStream_t stream);
 
+// Same, with other data pointers (the plan is not modified).
+int plan_enqueue_with(const Plan *p, const void *A, void *B, cudaStream_t stream);
+
 // The effective vector width and tile for the current pointers.
 int plan_vec_for_ptrs(const Plan *p);
 

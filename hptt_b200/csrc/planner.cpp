@@ -394,6 +394,8 @@ void finish_grid(const HpttProblem &p, HpttTile *t, const int64_t *tile_ext,
 void finish_tables(HpttTile *t) {
   fast_div_magic(static_cast<uint32_t>(t->R1 > 0 ? t->R1 : 1), &t->r1_mul, &t->r1_shr);
   fast_div_magic(static_cast<uint32_t>(t->R2 > 0 ? t->R2 : 1), &t->r2_mul, &t->r2_shr);
+  fast_div_magic(static_cast<uint32_t>(t->TX > 0 ? t->TX : 1), &t->tx_mul, &t->tx_shr);
+  fast_div_magic(static_cast<uint32_t>(t->TY > 0 ? t->TY : 1), &t->ty_mul, &t->ty_shr);
 }
 
 int choose_rows(const HpttProblem &p, const TileParams &tp, HpttTile *t) {
@@ -619,6 +621,29 @@ int choose_tile(const HpttProblem &p, const TileParams &tp, int update, HpttTile
     }
     tt = cdiv(n, cdiv(n, old));
   }
+  // Single-dim sides: round a chunked extent to a multiple of the threads
+  // per pass on its side (TY to R1, TX to R2), so every thread of an
+  // interior tile has the same iteration count and the kernel's predicate-
+  // free path applies ("even" tiles).
+  if (X.d.size() == 1 && Y.d.size() == 1) {
+    for (int round = 0; round < 2; ++round) {
+      for (int side = 0; side < 2; ++side) {
+        Side &S = side == 0 ? Y : X;
+        const int64_t n = p.n[S.d.back()];
+        int64_t &tt = S.t.back();
+        if (tt >= n) continue;
+        const int64_t other = side == 0 ? W * X.prod() : W * Y.prod();
+        const int64_t R = other > 0 ? tp.nt / other : 0;
+        if (R <= 1 || tt % R == 0) continue;
+        const int64_t old = tt;
+        tt = std::min<int64_t>(n, cdiv(old, R) * R);
+        if (tt < n && shape_ok(tp, W, X, Y, sz)) continue;
+        tt = (old / R) * R;
+        if (tt >= R && shape_ok(tp, W, X, Y, sz)) continue;
+        tt = old;
+      }
+    }
+  }
   if (!shape_ok(tp, W, X, Y, sz)) return ST_TOO_LARGE;
 
   t->W = static_cast<int32_t>(W);
@@ -651,6 +676,7 @@ int choose_tile(const HpttProblem &p, const TileParams &tp, int update, HpttTile
   t->J1 = static_cast<int32_t>(cdiv(t->TY, t->R1));
   t->R2 = t->nt / t->WTY;
   t->J2 = static_cast<int32_t>(cdiv(t->TX, t->R2));
+  t->even = (t->TY == t->R1 * t->J1 && t->TX == t->R2 * t->J2) ? 1 : 0;
   // row pitch with the fewest shared-memory bank conflicts
   TileMaps maps;
   tile_maps(p, *t, &maps);

@@ -1,0 +1,575 @@
+// Served form: a request loop that admits transposes as they arrive and runs
+// them on the GPU with continuous batching.
+//
+// A request names a plan (its tuned tile and offset tables stay resident on
+// the device) and optionally other device buffers of the plan's shape.  The
+// scheduler thread
+//   * admits queued requests in arrival order while the device bytes of the
+//     admitted, unfinished requests (A and B footprints) stay within the
+//     budget; a request whose output buffer an earlier unfinished request
+//     still writes waits in that buffer's own queue (and does not hold up
+//     later ones): admission is constant time per request;
+//   * batched mode: packs the admitted requests of one pass (at most
+//     max_batch) into one launch -- the batch layout and group kernels of the
+//     batched form -- on the next free stream of a pool of
+//     max_inflight_launches streams, so requests that arrive while earlier
+//     launches run are admitted into new launches that overlap them on the
+//     device;
+//   * per-call mode (the baseline): one plain exec per request, in arrival
+//     order, on one stream;
+//   * notices completions by polling each launch's event, stamps every
+//     request's latency (completion - submission, host steady clock) and
+//     frees its budget.
+// Every result equals the request's own plain exec: the same tile bodies and
+// arithmetic, and no two unfinished requests share an output buffer.
+// No reference counterpart: the reference is a library of synchronous plans.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <atomic>
+#include <chrono>
+#include <condition_variable>
+#include <cstring>
+#include <deque>
+#include <mutex>
+#include <new>
+#include <random>
+#include <thread>
+#include <unordered_map>
+#include <unordered_set>
+#include <vector>
+
+#include "../../include/hptt_cuda.h"
+#include "batch.h"
+#include "launch.h"
+#include "plan.h"
+#include "planner.h"
+
+namespace hptt_b200 {
+namespace {
+
+using Clock = std::chrono::steady_clock;
+constexpr uint32_t kServerMagic = 0x48505453u;  // "HPTS"
+
+struct Request {
+  uint64_t ticket = 0;
+  const Plan *plan = nullptr;
+  const void *A = nullptr;
+  void *B = nullptr;
+  uint64_t dev_bytes = 0;   // A and B footprints
+  uint64_t alg_bytes = 0;   // algorithmic bytes
+  Clock::time_point t_submit;
+};
+
+// One launch in flight (batched: a stream of the pool; per-call: one request
+// on the shared stream).
+struct Launch {
+  cudaStream_t stream = nullptr;
+  cudaEvent_t done = nullptr;
+  std::vector<Request> reqs;
+  bool busy = false;
+  // batched mode: device copies of the layout, pinned host staging
+  HpttBatchDesc *d_desc = nullptr;
+  HpttWork *d_work = nullptr;
+  uint32_t *d_counters = nullptr;
+  size_t desc_cap = 0, work_cap = 0, counter_cap = 0;
+  HpttBatchDesc *h_desc = nullptr;
+  HpttWork *h_work = nullptr;
+  size_t h_desc_cap = 0, h_work_cap = 0;
+};
+
+struct Server {
+  uint32_t magic = kServerMagic;
+  int device = 0;
+  int sms = 0;
+  hptt_cuda_serve_config cfg{};
+  std::thread worker;
+  std::atomic<bool> stop{false};
+
+  std::mutex mu;                       // guards everything below this line
+  std::condition_variable cv_submit;   // work arrived
+  std::condition_variable cv_done;     // a request finished
+  std::deque<Request> incoming;
+  uint64_t next_ticket = 1;
+  std::vector<int8_t> status;          // per ticket: -1 queued, else final status
+  uint64_t outstanding = 0;            // submitted and not finished
+  std::vector<float> lat_us;
+  uint64_t submitted = 0, completed = 0, failed = 0, launches = 0, bytes_done = 0;
+  uint64_t batched_requests = 0;
+  uint64_t peak_inflight_bytes = 0, peak_pending = 0;
+  Clock::time_point t_first_submit, t_last_done;
+  bool have_first = false;
+
+  // worker-owned.  Every unfinished request's output buffer is "claimed";
+  // `ready` holds requests whose output has no earlier unfinished request,
+  // in arrival order; `waiting[B]` holds later requests on a claimed B.
+  std::deque<Request> ready;
+  std::unordered_map<const void *, std::deque<Request>> waiting;
+  uint64_t n_waiting = 0;
+  std::vector<Launch> slots;
+  std::vector<size_t> free_slots;        // indices of idle slots
+  std::deque<size_t> inflight;           // busy slots in launch order
+  cudaStream_t shared_stream = nullptr;  // per-call mode
+  std::unordered_set<const void *> claimed;
+  uint64_t inflight_bytes = 0;
+};
+
+bool server_valid(const Server *s) { return s && s->magic == kServerMagic; }
+
+template <typename T>
+int grow_device(T **p, size_t *cap, size_t need) {
+  if (need <= *cap) return ST_OK;
+  if (*p) cudaFree(*p);
+  *p = nullptr;
+  *cap = 0;
+  const size_t n = std::max(need, static_cast<size_t>(64));
+  if (cudaMalloc(p, n * sizeof(T)) != cudaSuccess) {
+    cudaGetLastError();
+    return ST_ALLOC;
+  }
+  *cap = n;
+  return ST_OK;
+}
+
+template <typename T>
+int grow_pinned(T **p, size_t *cap, size_t need) {
+  if (need <= *cap) return ST_OK;
+  if (*p) cudaFreeHost(*p);
+  *p = nullptr;
+  *cap = 0;
+  const size_t n = std::max(need * 2, static_cast<size_t>(64));
+  if (cudaMallocHost(p, n * sizeof(T)) != cudaSuccess) {
+    cudaGetLastError();
+    return ST_ALLOC;
+  }
+  *cap = n;
+  return ST_OK;
+}
+
+uint64_t footprint_bytes(const Plan *p) {
+  const HpttProblem &q = p->args.p;
+  int64_t sa = 1, sb = 1;
+  for (int d = 0; d < q.rank; ++d) {
+    sa += (q.n[d] - 1) * q.sA[d];
+    sb += (q.n[d] - 1) * q.sB[d];
+  }
+  return static_cast<uint64_t>(sa + sb) * elem_bytes(q.dtype);
+}
+
+// Enqueue the requests of one launch.  Batched: one layout, uploaded from
+// pinned staging on the launch's stream, then the group kernels.  The
+// staging grows only when a launch needs more than the capacity reserved at
+// create (allocation calls can synchronise the device).
+int enqueue_launch(Server *s, Launch *L) {
+  if (s->cfg.per_call || L->reqs.size() == 1) {
+    // one request: its plain exec (no layout upload, one kernel)
+    const Request &r = L->reqs[0];
+    const int st = plan_enqueue_with(r.plan, r.A, r.B, L->stream);
+    if (st != ST_OK) return st;
+    return cudaEventRecord(L->done, L->stream) == cudaSuccess ? ST_OK : ST_CUDA;
+  }
+  std::vector<BatchEntry> entries(L->reqs.size());
+  for (size_t i = 0; i < L->reqs.size(); ++i) {
+    entries[i].plan = L->reqs[i].plan;
+    entries[i].A = L->reqs[i].A;
+    entries[i].B = L->reqs[i].B;
+  }
+  BatchLayout lay;
+  int st = batch_layout(entries, s->sms, &lay);
+  if (st != ST_OK) return st;
+  // the previous launch on this stream has finished (the slot was free), so
+  // its staging and device copies can be overwritten
+  if ((st = grow_device(&L->d_desc, &L->desc_cap, lay.desc.size())) != ST_OK ||
+      (st = grow_device(&L->d_work, &L->work_cap, lay.work.size())) != ST_OK ||
+      (st = grow_device(&L->d_counters, &L->counter_cap, lay.groups.size())) != ST_OK ||
+      (st = grow_pinned(&L->h_desc, &L->h_desc_cap, lay.desc.size())) != ST_OK ||
+      (st = grow_pinned(&L->h_work, &L->h_work_cap, lay.work.size())) != ST_OK)
+    return st;
+  std::memcpy(L->h_desc, lay.desc.data(), lay.desc.size() * sizeof(HpttBatchDesc));
+  std::memcpy(L->h_work, lay.work.data(), lay.work.size() * sizeof(HpttWork));
+  if (cudaMemcpyAsync(L->d_desc, L->h_desc, lay.desc.size() * sizeof(HpttBatchDesc),
+                      cudaMemcpyHostToDevice, L->stream) != cudaSuccess ||
+      (!lay.work.empty() &&
+       cudaMemcpyAsync(L->d_work, L->h_work, lay.work.size() * sizeof(HpttWork),
+                       cudaMemcpyHostToDevice, L->stream) != cudaSuccess))
+    return ST_CUDA;
+  st = batch_launch_groups(lay.groups, L->d_desc, L->d_work, L->d_counters, L->stream);
+  if (st != ST_OK) return st;
+  return cudaEventRecord(L->done, L->stream) == cudaSuccess ? ST_OK : ST_CUDA;
+}
+
+void finish_launch(Server *s, Launch *L, int st) {
+  const Clock::time_point now = Clock::now();
+  for (const Request &r : L->reqs) {
+    s->inflight_bytes -= r.dev_bytes;
+    // the next request on this output (if any) becomes ready
+    auto w = s->waiting.find(r.B);
+    if (w != s->waiting.end() && !w->second.empty()) {
+      s->ready.push_back(w->second.front());
+      w->second.pop_front();
+      --s->n_waiting;
+      if (w->second.empty()) s->waiting.erase(w);
+    } else {
+      s->claimed.erase(r.B);
+    }
+  }
+  {
+    std::lock_guard<std::mutex> lk(s->mu);
+    for (const Request &r : L->reqs) {
+      s->status[r.ticket] = static_cast<int8_t>(st);
+      --s->outstanding;
+      if (st == ST_OK) {
+        ++s->completed;
+        s->bytes_done += r.alg_bytes;
+        s->lat_us.push_back(static_cast<float>(
+            std::chrono::duration<double, std::micro>(now - r.t_submit).count()));
+      } else {
+        ++s->failed;
+      }
+    }
+    s->t_last_done = now;
+  }
+  L->reqs.clear();
+  L->busy = false;
+  s->cv_done.notify_all();
+}
+
+// A new request: ready when its output is free, else queued behind it.
+void enqueue_request(Server *s, const Request &r) {
+  if (s->claimed.insert(r.B).second) {
+    s->ready.push_back(r);
+  } else {
+    s->waiting[r.B].push_back(r);
+    ++s->n_waiting;
+  }
+}
+
+// Admit ready requests into launch L in arrival order while they fit the
+// budget.  Returns the number admitted.
+size_t admit(Server *s, Launch *L, size_t max_n) {
+  size_t taken = 0;
+  while (taken < max_n && !s->ready.empty()) {
+    const Request &r = s->ready.front();
+    if (s->inflight_bytes + r.dev_bytes > s->cfg.budget_bytes) break;
+    s->inflight_bytes += r.dev_bytes;
+    L->reqs.push_back(r);
+    s->ready.pop_front();
+    ++taken;
+  }
+  return taken;
+}
+
+void worker_main(Server *s) {
+  cudaSetDevice(s->device);
+  const size_t max_batch = s->cfg.per_call ? 1 : std::max<uint32_t>(1, s->cfg.max_batch);
+  for (;;) {
+    {
+      std::lock_guard<std::mutex> lk(s->mu);
+      while (!s->incoming.empty()) {
+        enqueue_request(s, s->incoming.front());
+        s->incoming.pop_front();
+      }
+      s->peak_pending =
+          std::max<uint64_t>(s->peak_pending, s->ready.size() + s->n_waiting);
+    }
+    bool progress = false;
+    // completions: per-call launches share one stream and finish in order,
+    // so only the oldest is polled; batched launches (a few streams) each
+    for (auto it = s->inflight.begin(); it != s->inflight.end();) {
+      Launch &L = s->slots[*it];
+      const cudaError_t q = cudaEventQuery(L.done);
+      if (q == cudaErrorNotReady) {
+        if (s->cfg.per_call) break;
+        ++it;
+        continue;
+      }
+      if (q != cudaSuccess) cudaGetLastError();
+      finish_launch(s, &L, q == cudaSuccess ? ST_OK : ST_CUDA);
+      s->free_slots.push_back(*it);
+      it = s->inflight.erase(it);
+      progress = true;
+    }
+    // admissions: every idle slot takes the next admissible requests
+    while (!s->free_slots.empty() && !s->ready.empty()) {
+      const size_t k = s->free_slots.back();
+      Launch &L = s->slots[k];
+      if (admit(s, &L, max_batch) == 0) break;
+      s->free_slots.pop_back();
+      {
+        std::lock_guard<std::mutex> lk(s->mu);
+        s->peak_inflight_bytes = std::max(s->peak_inflight_bytes, s->inflight_bytes);
+        ++s->launches;
+        s->batched_requests += L.reqs.size();
+      }
+      L.busy = true;
+      const int st = enqueue_launch(s, &L);
+      if (st != ST_OK) {
+        cudaGetLastError();
+        finish_launch(s, &L, st);
+        s->free_slots.push_back(k);
+      } else {
+        s->inflight.push_back(k);
+      }
+      progress = true;
+    }
+    if (progress) continue;
+    std::unique_lock<std::mutex> lk(s->mu);
+    const bool busy = !s->inflight.empty();
+    if (s->stop && s->incoming.empty() && s->ready.empty() && s->n_waiting == 0 && !busy)
+      break;
+    if (!busy && s->incoming.empty()) {
+      // idle: sleep until a submission (or stop)
+      s->cv_submit.wait_for(lk, std::chrono::milliseconds(5));
+    } else {
+      lk.unlock();
+      std::this_thread::yield();
+    }
+  }
+}
+
+void free_slots(Server *s) {
+  for (Launch &L : s->slots) {
+    if (L.done) cudaEventDestroy(L.done);
+    if (L.stream && L.stream != s->shared_stream) cudaStreamDestroy(L.stream);
+    if (L.d_desc) cudaFree(L.d_desc);
+    if (L.d_work) cudaFree(L.d_work);
+    if (L.d_counters) cudaFree(L.d_counters);
+    if (L.h_desc) cudaFreeHost(L.h_desc);
+    if (L.h_work) cudaFreeHost(L.h_work);
+  }
+  s->slots.clear();
+  if (s->shared_stream) cudaStreamDestroy(s->shared_stream);
+  s->shared_stream = nullptr;
+}
+
+double percentile(std::vector<float> &v, double q) {
+  if (v.empty()) return 0.0;
+  const size_t k = std::min(v.size() - 1, static_cast<size_t>(q * (v.size() - 1) + 0.5));
+  std::nth_element(v.begin(), v.begin() + k, v.end());
+  return v[k];
+}
+
+}  // namespace
+}  // namespace hptt_b200
+
+using namespace hptt_b200;
+
+extern "C" {
+
+int hptt_cuda_server_create(const hptt_cuda_serve_config *cfg, hptt_cuda_server_t *server) {
+  if (!server) return HPTT_ERR_HANDLE;
+  *server = nullptr;
+  if (!cfg || cfg->budget_bytes == 0 || cfg->max_inflight_launches == 0 ||
+      (!cfg->per_call && cfg->max_batch == 0))
+    return HPTT_ERR_SIZE_VALUE;
+  Server *s = new (std::nothrow) Server();
+  if (!s) return HPTT_ERR_ALLOC;
+  s->cfg = *cfg;
+  if (cudaGetDevice(&s->device) != cudaSuccess ||
+      cudaDeviceGetAttribute(&s->sms, cudaDevAttrMultiProcessorCount, s->device) !=
+          cudaSuccess) {
+    delete s;
+    return HPTT_ERR_NO_DEVICE;
+  }
+  int st = ST_OK;
+  if (cfg->per_call &&
+      cudaStreamCreateWithFlags(&s->shared_stream, cudaStreamNonBlocking) != cudaSuccess)
+    st = ST_CUDA;
+  s->slots.resize(cfg->max_inflight_launches);
+  for (Launch &L : s->slots) {
+    if (st != ST_OK) break;
+    if (cfg->per_call)
+      L.stream = s->shared_stream;
+    else if (cudaStreamCreateWithFlags(&L.stream, cudaStreamNonBlocking) != cudaSuccess)
+      st = ST_CUDA;
+    if (st == ST_OK && cudaEventCreateWithFlags(&L.done, cudaEventDisableTiming) != cudaSuccess)
+      st = ST_CUDA;
+  }
+  if (st != ST_OK) {
+    cudaGetLastError();
+    free_slots(s);
+    delete s;
+    return st;
+  }
+  // batched mode: reserve the staging every launch needs, so the scheduler
+  // loop does not allocate (cudaMalloc/cudaFree can synchronise the device)
+  if (!cfg->per_call) {
+    const size_t nd = cfg->max_batch, nw = std::max<size_t>(65536, 64 * nd);
+    for (Launch &L : s->slots) {
+      if (st != ST_OK) break;
+      if ((st = grow_device(&L.d_desc, &L.desc_cap, nd)) != ST_OK ||
+          (st = grow_device(&L.d_work, &L.work_cap, nw)) != ST_OK ||
+          (st = grow_device(&L.d_counters, &L.counter_cap, 128)) != ST_OK ||
+          (st = grow_pinned(&L.h_desc, &L.h_desc_cap, nd)) != ST_OK ||
+          (st = grow_pinned(&L.h_work, &L.h_work_cap, nw)) != ST_OK)
+        break;
+    }
+    if (st != ST_OK) {
+      free_slots(s);
+      delete s;
+      return st;
+    }
+  }
+  for (size_t k = s->slots.size(); k-- > 0;) s->free_slots.push_back(k);
+  s->status.assign(1, 0);
+  s->worker = std::thread(worker_main, s);
+  *server = reinterpret_cast<hptt_cuda_server_t>(s);
+  return HPTT_OK;
+}
+
+int hptt_cuda_server_submit(hptt_cuda_server_t server, hptt_cuda_plan_t plan, const void *in,
+                            void *out, uint64_t *ticket) {
+  Server *s = reinterpret_cast<Server *>(server);
+  if (!server_valid(s)) return HPTT_ERR_HANDLE;
+  Plan *p = reinterpret_cast<Plan *>(plan);
+  if (!plan_valid(p) || p->device != s->device) return HPTT_ERR_HANDLE;
+  if ((in == nullptr) != (out == nullptr)) return HPTT_ERR_NULL_DATA;
+  Request r;
+  r.plan = p;
+  r.A = in ? in : p->args.A;
+  r.B = in ? out : p->args.B;
+  if (!r.A || !r.B) return HPTT_ERR_NULL_DATA;
+  r.dev_bytes = footprint_bytes(p);
+  if (r.dev_bytes > s->cfg.budget_bytes) return HPTT_ERR_BUDGET;
+  r.alg_bytes = p->elements * static_cast<uint64_t>(elem_bytes(p->args.p.dtype)) *
+                (p->args.update ? 3u : 2u);
+  r.t_submit = Clock::now();
+  {
+    std::lock_guard<std::mutex> lk(s->mu);
+    if (s->stop) return HPTT_ERR_HANDLE;
+    r.ticket = s->next_ticket++;
+    s->status.push_back(-1);
+    ++s->outstanding;
+    ++s->submitted;
+    if (!s->have_first) {
+      s->have_first = true;
+      s->t_first_submit = r.t_submit;
+    }
+    s->incoming.push_back(r);
+  }
+  s->cv_submit.notify_one();
+  if (ticket) *ticket = r.ticket;
+  return HPTT_OK;
+}
+
+int hptt_cuda_server_wait(hptt_cuda_server_t server, uint64_t ticket, double timeout_s) {
+  Server *s = reinterpret_cast<Server *>(server);
+  if (!server_valid(s)) return HPTT_ERR_HANDLE;
+  std::unique_lock<std::mutex> lk(s->mu);
+  if (ticket == 0 || ticket >= s->next_ticket) return HPTT_ERR_HANDLE;
+  const bool ok = s->cv_done.wait_for(lk, std::chrono::duration<double>(timeout_s),
+                                      [&] { return s->status[ticket] >= 0; });
+  return ok ? s->status[ticket] : HPTT_ERR_TIMEOUT;
+}
+
+int hptt_cuda_server_drain(hptt_cuda_server_t server, double timeout_s) {
+  Server *s = reinterpret_cast<Server *>(server);
+  if (!server_valid(s)) return HPTT_ERR_HANDLE;
+  std::unique_lock<std::mutex> lk(s->mu);
+  const bool ok = s->cv_done.wait_for(lk, std::chrono::duration<double>(timeout_s),
+                                      [&] { return s->outstanding == 0; });
+  if (!ok) return HPTT_ERR_TIMEOUT;
+  return s->failed ? HPTT_ERR_CUDA : HPTT_OK;
+}
+
+int hptt_cuda_server_stats(hptt_cuda_server_t server, hptt_cuda_serve_stats *out) {
+  Server *s = reinterpret_cast<Server *>(server);
+  if (!server_valid(s) || !out) return HPTT_ERR_HANDLE;
+  std::vector<float> lat;
+  std::memset(out, 0, sizeof(*out));
+  {
+    std::lock_guard<std::mutex> lk(s->mu);
+    lat = s->lat_us;
+    out->submitted = s->submitted;
+    out->completed = s->completed;
+    out->failed = s->failed;
+    out->launches = s->launches;
+    out->bytes = s->bytes_done;
+    out->peak_inflight_bytes = s->peak_inflight_bytes;
+    out->peak_pending = s->peak_pending;
+    out->mean_batch = s->launches ? static_cast<double>(s->batched_requests) / s->launches : 0;
+    if (s->have_first && s->completed)
+      out->elapsed_s = std::chrono::duration<double>(s->t_last_done - s->t_first_submit).count();
+  }
+  if (out->elapsed_s > 0) {
+    out->throughput_rps = out->completed / out->elapsed_s;
+    out->gbs = out->bytes / out->elapsed_s / 1e9;
+  }
+  if (!lat.empty()) {
+    double sum = 0, mx = 0;
+    for (float v : lat) {
+      sum += v;
+      mx = std::max<double>(mx, v);
+    }
+    out->lat_mean_us = sum / lat.size();
+    out->lat_max_us = mx;
+    out->lat_p50_us = percentile(lat, 0.50);
+    out->lat_p99_us = percentile(lat, 0.99);
+    out->lat_p999_us = percentile(lat, 0.999);
+  }
+  return HPTT_OK;
+}
+
+int hptt_cuda_server_reset_stats(hptt_cuda_server_t server) {
+  Server *s = reinterpret_cast<Server *>(server);
+  if (!server_valid(s)) return HPTT_ERR_HANDLE;
+  std::lock_guard<std::mutex> lk(s->mu);
+  if (s->outstanding) return HPTT_ERR_BUSY;
+  s->lat_us.clear();
+  s->submitted = s->completed = s->failed = s->launches = s->bytes_done = 0;
+  s->batched_requests = 0;
+  s->peak_inflight_bytes = s->peak_pending = 0;
+  s->have_first = false;
+  return HPTT_OK;
+}
+
+int hptt_cuda_server_destroy(hptt_cuda_server_t server) {
+  Server *s = reinterpret_cast<Server *>(server);
+  if (!server_valid(s)) return HPTT_ERR_HANDLE;
+  {
+    std::lock_guard<std::mutex> lk(s->mu);
+    s->stop = true;
+  }
+  s->cv_submit.notify_all();
+  if (s->worker.joinable()) s->worker.join();
+  free_slots(s);
+  s->magic = 0;
+  delete s;
+  return HPTT_OK;
+}
+
+int hptt_cuda_server_run_poisson(hptt_cuda_server_t server, const hptt_cuda_plan_t *pool,
+                                 uint32_t pool_size, double rate, double seconds,
+                                 uint64_t seed, double drain_timeout_s,
+                                 hptt_cuda_serve_stats *stats) {
+  Server *s = reinterpret_cast<Server *>(server);
+  if (!server_valid(s)) return HPTT_ERR_HANDLE;
+  if (!pool || pool_size == 0 || !(rate > 0) || !(seconds > 0)) return HPTT_ERR_SIZE_VALUE;
+  int st = hptt_cuda_server_reset_stats(server);
+  if (st != HPTT_OK) return st;
+  std::mt19937_64 rng(seed);
+  std::exponential_distribution<double> gap(rate);
+  std::uniform_int_distribution<uint32_t> pick(0, pool_size - 1);
+  const Clock::time_point t0 = Clock::now();
+  double t_next = 0.0;
+  while (t_next < seconds) {
+    const Clock::time_point due =
+        t0 + std::chrono::duration_cast<Clock::duration>(std::chrono::duration<double>(t_next));
+    for (;;) {
+      const Clock::time_point now = Clock::now();
+      if (now >= due) break;
+      if (due - now > std::chrono::microseconds(200))
+        std::this_thread::sleep_for(std::chrono::microseconds(50));
+      else
+        std::this_thread::yield();
+    }
+    st = hptt_cuda_server_submit(server, pool[pick(rng)], nullptr, nullptr, nullptr);
+    if (st != HPTT_OK) return st;
+    t_next += gap(rng);
+  }
+  st = hptt_cuda_server_drain(server, drain_timeout_s);
+  const int st2 = hptt_cuda_server_stats(server, stats);
+  return st != HPTT_OK ? st : st2;
+}
+
+}  // extern "C"

@@ -86,10 +86,24 @@ int replay_tile(const HpttProblem &P, const HpttTile &T, int update, const Layou
       if (static_cast<int64_t>(tabX[q].off) != q * sX || tabX[q].c != (T.xc >= 0 ? q : 0))
         return 120;
   }
+  // single-dim sides with W == 1: the kernel computes the per-thread
+  // constants from the thread index; they must equal the table's
+  if (!T.big_offsets && T.nx == 1 && T.ny == 1 && T.W == 1) {
+    for (int t = 0; t < T.nt; ++t) {
+      const HpttThr a = thread_consts_1d(P, T, t), &b = thr[t];
+      if (a.q0 != b.q0 || a.qs0 != b.qs0 || a.inE != b.inE || a.outE2 != b.outE2 ||
+          a.sme != b.sme || a.sme2 != b.sme2 || a.cxe != b.cxe || a.cye2 != b.cye2 ||
+          a.active != b.active)
+        return 131;
+    }
+  }
   const int64_t smem_elems = static_cast<int64_t>(T.TY) * T.LD;
   std::vector<int64_t> slot(smem_elems);
   // the kernel's single-dim-side variants (kernels.cu: pick_tile)
   const bool ly = !T.big_offsets && T.ny <= 1, lx = !T.big_offsets && T.nx <= 1;
+  // the interior fast path (kernels.cuh) assumes every loading thread has
+  // J1 rows and every storing thread J2 columns
+  if (T.even && !(T.TY == T.R1 * T.J1 && T.TX == T.R2 * T.J2)) return 130;
   // the kernel indexes single-dim sides as q * stride in 32-bit ints
   if (ly && T.ny == 1 && T.TY > 1 && P.sA[T.yd[0]] > 0x7fffffffLL) return 128;
   if (lx && T.nx == 1 && T.TX > 1 && P.sB[T.xd[0]] > 0x7fffffffLL) return 129;

@@ -200,6 +200,103 @@ int hptt_cuda_transpose_noalloc(int dtype, uint32_t rank, const uint32_t *in_siz
  * the reference. */
 size_t hptt_cuda_noalloc_table_bytes(void);
 
+/*
+ * Batched form: many plans in one graph launch.  No reference counterpart:
+ * the reference runs each plan's exec on its own
+ * (inc/hptt/cgraph/cgraph_trans.tcc:27-48); a batch replaces a loop of those
+ * calls.
+ *
+ * A batch snapshots each plan's launch arguments (problem, tuned tile,
+ * offset tables, data pointers, scalars) into a device descriptor table and
+ * splits every plan's tiles into work items, grouped by tile body (element
+ * storage, arithmetic, B read, tile shape).  One persistent kernel per group
+ * takes its items from an atomic counter; a CUDA graph built at create holds
+ * the counter reset and every group kernel as independent nodes, so the
+ * groups run side by side and one graph launch runs the batch.  Results are
+ * bit-identical to each plan's own exec.  The plans must outlive the batch
+ * (their offset tables are shared, not copied), and no plan's output may
+ * overlap another plan's input or output (entries run concurrently, in no
+ * fixed order).
+ *   create    build descriptors, work list and graph (synchronous uploads)
+ *   refresh   re-read every plan's pointers and scalars after reset_data /
+ *             set_coef on it; rebuilds the graph only if the launch shape
+ *             changed
+ *   exec      enqueue one run on a stream (cudaStream_t as void*; NULL =
+ *             legacy default stream)
+ *   info      algorithmic bytes of one exec, work items, kernels per exec
+ */
+typedef struct hptt_cuda_batch_s *hptt_cuda_batch_t;
+int hptt_cuda_batch_create(const hptt_cuda_plan_t *plans, uint32_t count,
+                           hptt_cuda_batch_t *batch);
+int hptt_cuda_batch_refresh(hptt_cuda_batch_t batch);
+int hptt_cuda_batch_exec(hptt_cuda_batch_t batch, void *stream);
+int hptt_cuda_batch_info(hptt_cuda_batch_t batch, uint64_t *bytes, uint32_t *work_items,
+                         uint32_t *kernels);
+int hptt_cuda_batch_destroy(hptt_cuda_batch_t batch);
+
+/* The per-call form a batch is compared with: exactly one
+ * hptt_cuda_plan_exec_on(plans[i], stream) per plan, in order, from one C
+ * loop (no interpreter between calls).  Reference counterpart: a caller's
+ * loop of plan->exec() (inc/hptt/impl/hptt_trans.h:26). */
+int hptt_cuda_plan_exec_many(const hptt_cuda_plan_t *plans, uint32_t count, void *stream);
+
+/*
+ * Served form: a request loop with continuous batching.  No reference
+ * counterpart (the reference is a library of synchronous plans).
+ *
+ * A request names a plan -- its tuned tile and offset tables stay resident --
+ * and optionally other device buffers of the plan's shape (in/out both NULL:
+ * the plan's own).  A scheduler thread admits queued requests in arrival
+ * order while the device bytes (A and B footprints) of admitted, unfinished
+ * requests stay within budget_bytes; a request whose output buffer an
+ * earlier unfinished request still writes waits without holding up later
+ * ones.  Batched mode packs each pass's admissions (at most max_batch) into
+ * one launch of the batched form's group kernels on a free stream of a pool
+ * of max_inflight_launches streams, so arrivals during earlier launches run
+ * in new launches that overlap them.  per_call != 0 is the baseline: one
+ * plain exec per request, in arrival order, on one stream, with up to
+ * max_inflight_launches requests enqueued at once.  Completions are found by
+ * polling events; a request's latency is completion minus submission on the
+ * host's steady clock.  Each result equals the request's own plain exec.
+ *   submit      queue a request (non-blocking); *ticket identifies it.
+ *               HPTT_ERR_BUDGET if it alone exceeds the budget.
+ *   wait        until that request finished (its status) or timeout
+ *               (HPTT_ERR_TIMEOUT)
+ *   drain       until every submitted request finished
+ *   stats       counters and latency percentiles since the last reset
+ *   reset_stats only when nothing is outstanding (else HPTT_ERR_BUSY)
+ *   run_poisson open-loop load: arrivals with exponential gaps at `rate`
+ *               per second for `seconds`, each a uniformly drawn plan of
+ *               `pool` on its own buffers; then drain; fills *stats
+ *   destroy     finishes everything queued, then frees the server
+ */
+typedef struct hptt_cuda_server_s *hptt_cuda_server_t;
+typedef struct {
+  uint64_t budget_bytes;
+  uint32_t max_inflight_launches;
+  uint32_t max_batch;
+  int32_t per_call;
+  int32_t reserved;
+} hptt_cuda_serve_config;
+typedef struct {
+  uint64_t submitted, completed, failed, launches, bytes;
+  uint64_t peak_inflight_bytes, peak_pending;
+  double elapsed_s, throughput_rps, gbs, mean_batch;
+  double lat_mean_us, lat_p50_us, lat_p99_us, lat_p999_us, lat_max_us;
+} hptt_cuda_serve_stats;
+int hptt_cuda_server_create(const hptt_cuda_serve_config *cfg, hptt_cuda_server_t *server);
+int hptt_cuda_server_submit(hptt_cuda_server_t server, hptt_cuda_plan_t plan, const void *in,
+                            void *out, uint64_t *ticket);
+int hptt_cuda_server_wait(hptt_cuda_server_t server, uint64_t ticket, double timeout_s);
+int hptt_cuda_server_drain(hptt_cuda_server_t server, double timeout_s);
+int hptt_cuda_server_stats(hptt_cuda_server_t server, hptt_cuda_serve_stats *stats);
+int hptt_cuda_server_reset_stats(hptt_cuda_server_t server);
+int hptt_cuda_server_run_poisson(hptt_cuda_server_t server, const hptt_cuda_plan_t *pool,
+                                 uint32_t pool_size, double rate, double seconds,
+                                 uint64_t seed, double drain_timeout_s,
+                                 hptt_cuda_serve_stats *stats);
+int hptt_cuda_server_destroy(hptt_cuda_server_t server);
+
 /* Autotune cache: the tile parameters the tuner picked, one entry per
  * (GPU name, dtype, fused rank, fused perm, size class, B read).  Plans
  * created with tuning_timeout == 0 use a matching entry instead of the
