@@ -645,6 +645,16 @@ int choose_tile(const HpttProblem &p, const TileParams &tp, int update, HpttTile
     }
   }
   if (!shape_ok(tp, W, X, Y, sz)) return ST_TOO_LARGE;
+  // A trailing dim with tile extent 1 adds nothing to the tile (the grid
+  // steps through it either way) but would keep the side off the single-dim
+  // kernel path: drop it.
+  for (Side *S : {&X, &Y}) {
+    while (S->d.size() > 1 && S->t.back() == 1) {
+      in_tile[S->d.back()] = false;
+      S->d.pop_back();
+      S->t.pop_back();
+    }
+  }
 
   t->W = static_cast<int32_t>(W);
   t->nx = static_cast<int32_t>(X.d.size());

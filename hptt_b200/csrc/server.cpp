@@ -85,6 +85,7 @@ struct Server {
   hptt_cuda_serve_config cfg{};
   std::thread worker;
   std::atomic<bool> stop{false};
+  std::atomic<bool> abandon{false};  // destroy: fail what has not launched
 
   std::mutex mu;                       // guards everything below this line
   std::condition_variable cv_submit;   // work arrived
@@ -259,6 +260,23 @@ size_t admit(Server *s, Launch *L, size_t max_n) {
   return taken;
 }
 
+void fail_queued(Server *s) {
+  std::vector<Request> dropped(s->ready.begin(), s->ready.end());
+  s->ready.clear();
+  for (auto &kv : s->waiting)
+    for (const Request &r : kv.second) dropped.push_back(r);
+  s->waiting.clear();
+  s->n_waiting = 0;
+  if (dropped.empty()) return;
+  std::lock_guard<std::mutex> lk(s->mu);
+  for (const Request &r : dropped) {
+    s->status[r.ticket] = static_cast<int8_t>(ST_TIMEOUT);
+    --s->outstanding;
+    ++s->failed;
+  }
+  s->cv_done.notify_all();
+}
+
 void worker_main(Server *s) {
   cudaSetDevice(s->device);
   const size_t max_batch = s->cfg.per_call ? 1 : std::max<uint32_t>(1, s->cfg.max_batch);
@@ -273,6 +291,11 @@ void worker_main(Server *s) {
           std::max<uint64_t>(s->peak_pending, s->ready.size() + s->n_waiting);
     }
     bool progress = false;
+    if (s->abandon) {
+      // destroy gave up waiting: queued requests that never launched fail
+      // (launches already on the GPU still finish below)
+      fail_queued(s);
+    }
     // completions: per-call launches share one stream and finish in order,
     // so only the oldest is polled; batched launches (a few streams) each
     for (auto it = s->inflight.begin(); it != s->inflight.end();) {
@@ -531,6 +554,9 @@ int hptt_cuda_server_destroy(hptt_cuda_server_t server) {
     s->stop = true;
   }
   s->cv_submit.notify_all();
+  // finish what is queued, within a bound; then fail what has not launched
+  // (launched kernels are bounded, so the join below always returns)
+  if (hptt_cuda_server_drain(server, 60.0) == HPTT_ERR_TIMEOUT) s->abandon = true;
   if (s->worker.joinable()) s->worker.join();
   free_slots(s);
   s->magic = 0;
