@@ -8,6 +8,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
+#include <cstring>
 #include <fstream>
 #include <map>
 #include <mutex>
@@ -36,8 +37,9 @@ std::string gpu_name() {
 
 const char *env_path() { return std::getenv("HPTT_B200_TUNE_CACHE"); }
 
-// Cache file: one line per key, "key|run vmin smem rows_min y_first iters"
-// (a line without the last field keeps max_iters = 0).
+// Cache file: one line per key,
+// "key|run vmin smem rows_min y_first iters full_side"
+// (missing trailing fields read as 0).
 void read_cache_stream(std::istream &f) {
   std::string line;
   while (std::getline(f, line)) {
@@ -48,6 +50,7 @@ void read_cache_stream(std::istream &f) {
     if (v >> tp.run_bytes >> tp.vmin_bytes >> tp.smem_bytes >> tp.rows_min_bytes >>
         tp.y_first) {
       if (!(v >> tp.max_iters)) tp.max_iters = 0;
+      if (!(v >> tp.full_side)) tp.full_side = 0;
       g_cache[line.substr(0, bar)] = tp;
     }
   }
@@ -68,26 +71,31 @@ int write_cache(const char *path) {
   for (const auto &kv : g_cache)
     f << kv.first << "|" << kv.second.run_bytes << " " << kv.second.vmin_bytes << " "
       << kv.second.smem_bytes << " " << kv.second.rows_min_bytes << " "
-      << kv.second.y_first << " " << kv.second.max_iters << "\n";
+      << kv.second.y_first << " " << kv.second.max_iters << " " << kv.second.full_side
+      << "\n";
   return ST_OK;
 }
 
 // Candidate tile parameters: which side is chosen first, the contiguous run
-// wanted on each side, the minimum tile volume, and the per-thread
-// iterations (the kernel's limit or half of it: smaller tiles, more CTAs).
+// wanted on each side, the minimum tile volume, the per-thread iterations
+// (the kernel's limit or half of it: smaller tiles, more CTAs), and whether a
+// single-dim side takes its whole extent.  Candidates that plan the same tile
+// as an earlier one are not timed again.
 std::vector<TileParams> candidates(int elem_size) {
   std::vector<TileParams> c;
-  for (int iters : {0, hptt_jmax_tile(elem_size) / 2})
-    for (int yf : {0, 1})
-      for (int run : {256, 128, 512})
-        for (int vmin : {16384, 8192}) {
-          TileParams tp;
-          tp.y_first = yf;
-          tp.run_bytes = run;
-          tp.vmin_bytes = vmin;
-          tp.max_iters = iters;
-          c.push_back(tp);
-        }
+  for (int full : {0, 1, 2})
+    for (int iters : {0, hptt_jmax_tile(elem_size) / 2})
+      for (int yf : {0, 1})
+        for (int run : {256, 128, 512})
+          for (int vmin : {16384, 8192}) {
+            TileParams tp;
+            tp.y_first = yf;
+            tp.run_bytes = run;
+            tp.vmin_bytes = vmin;
+            tp.max_iters = iters;
+            tp.full_side = full;
+            c.push_back(tp);
+          }
   return c;
 }
 
@@ -138,6 +146,7 @@ int autotune(Plan *p, double timeout, TileParams *best) {
   bool found = false;
   void *user_B = p->args.B;
   p->args.B = scratch;
+  std::vector<HpttTile> timed;  // tiles already timed (identical plans skip)
   for (const TileParams &tp : candidates(elem_bytes(p->args.p.dtype))) {
     if (st != ST_OK) break;
     if (timeout > 0) {
@@ -145,6 +154,11 @@ int autotune(Plan *p, double timeout, TileParams *best) {
       if (el > timeout) break;
     }
     if (plan_tiles(p, tp) != ST_OK) continue;
+    bool seen = false;
+    for (const HpttTile &t : timed)
+      if (std::memcmp(&t, &p->args.t, sizeof(HpttTile)) == 0) seen = true;
+    if (seen) continue;
+    timed.push_back(p->args.t);
     if (plan_enqueue(p, s) != ST_OK) continue;  // warm-up
     float ms_best = 1e30f;
     for (int r = 0; r < 3; ++r) {

@@ -286,20 +286,25 @@ int batch_layout(const std::vector<BatchEntry> &entries, int sms, BatchLayout *L
   return ST_OK;
 }
 
+int batch_launch_group(const BatchGroup &g, const HpttBatchDesc *d_desc, const HpttWork *d_work,
+                       uint32_t *d_counter, cudaStream_t stream) {
+  const void *fn = kernel_of(g.body);
+  uint32_t begin = g.begin, end = g.end;
+  void *params[] = {&d_desc, &d_work, &begin, &end, &d_counter};
+  return cudaLaunchKernel(fn, dim3(g.grid), dim3(kNT), params,
+                          static_cast<size_t>(g.smem_bytes), stream) == cudaSuccess
+             ? ST_OK
+             : ST_CUDA;
+}
+
 int batch_launch_groups(const std::vector<BatchGroup> &groups, const HpttBatchDesc *d_desc,
                         const HpttWork *d_work, uint32_t *d_counters, cudaStream_t stream) {
   if (groups.empty()) return ST_OK;
   if (cudaMemsetAsync(d_counters, 0, groups.size() * sizeof(uint32_t), stream) != cudaSuccess)
     return ST_CUDA;
   for (size_t gi = 0; gi < groups.size(); ++gi) {
-    const BatchGroup &g = groups[gi];
-    const void *fn = kernel_of(g.body);
-    uint32_t begin = g.begin, end = g.end;
-    uint32_t *counter = d_counters + gi;
-    void *params[] = {&d_desc, &d_work, &begin, &end, &counter};
-    if (cudaLaunchKernel(fn, dim3(g.grid), dim3(kNT), params,
-                         static_cast<size_t>(g.smem_bytes), stream) != cudaSuccess)
-      return ST_CUDA;
+    const int st = batch_launch_group(groups[gi], d_desc, d_work, d_counters + gi, stream);
+    if (st != ST_OK) return st;
   }
   return ST_OK;
 }

@@ -87,6 +87,10 @@ struct BatchLayout {
 };
 int batch_layout(const std::vector<BatchEntry> &entries, int sms, BatchLayout *layout);
 
+// Launch one group kernel (its counter must be zero).
+int batch_launch_group(const BatchGroup &g, const HpttBatchDesc *d_desc, const HpttWork *d_work,
+                       uint32_t *d_counter, cudaStream_t stream);
+
 // Reset the group counters and launch every group kernel on `stream` (one
 // after another), reading descriptors and work items from device memory.
 int batch_launch_groups(const std::vector<BatchGroup> &groups, const HpttBatchDesc *d_desc,

@@ -73,6 +73,16 @@ struct HpttTile {
   uint32_t gmul[HPTT_MAX_RANK];  // fast division by gcnt: q = umulhi(n, gmul) >> gshr
   int32_t gshr[HPTT_MAX_RANK];   // (gmul = 0 encodes gcnt == 1)
   int32_t gstep[HPTT_MAX_RANK];
+  // per grid level, folded for the device (static-offset parameter reads):
+  // the origin advances by c * gsa[g] in A and c * gsb[g] in B; gn = extent
+  // of dim gd[g]; gflag bit 0 / 1: gd[g] is the chunked X / Y dim (xc / yc,
+  // for KIND_ROWS wc / yc)
+  int64_t gsa[HPTT_MAX_RANK], gsb[HPTT_MAX_RANK];
+  int64_t gn[HPTT_MAX_RANK];
+  int32_t gflag[HPTT_MAX_RANK];
+  // single-dim sides: strides of the X dim in A and B, of the Y dim in A
+  // and B (0 when that side has no dim or several)
+  int64_t sxa, sxb, sya, syb;
   uint32_t num_tiles;
   int32_t big_offsets;        // 1 when in-tile offsets need 64 bits
   int32_t smem_bytes;         // dynamic shared memory for one CTA

@@ -15,10 +15,9 @@ constexpr int kNT = 256;
 // One CTA per tile.  The arguments live in the parameter space
 // (__grid_constant__) and are read through a const reference.  Register
 // budgets: 6 resident CTAs per SM for the copy/scale tiles (the shared-memory
-// limit at 32 KB a tile), 8 for table-free ones with elements of at most 8
-// bytes (32 registers), 4 when B is read too.
+// limit at 32 KB a tile), 4 when B is read too.
 template <typename E, int MODE, bool UPD, typename OffT, bool LX, bool LY>
-__global__ void __launch_bounds__(kNT, UPD ? 4 : (LX && LY && sizeof(E) <= 8 ? 8 : 6)) k_tile(const __grid_constant__ HpttArgs args) {
+__global__ void __launch_bounds__(kNT, UPD ? 4 : 6) k_tile(const __grid_constant__ HpttArgs args) {
   extern __shared__ __align__(16) unsigned char smem[];
   const Scal sc{args.alpha[0], args.alpha[1], args.beta[0], args.beta[1]};
   const Op<E, MODE, UPD> op(sc);

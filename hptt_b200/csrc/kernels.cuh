@@ -85,28 +85,34 @@ struct TileOrigin {
   int remY;        // extent left along the chunked Y dim, capped
 };
 
+// Origin of tile `tile`: a mixed-radix decode over the grid levels, each
+// level's steps folded by the planner (gsa, gsb, gn, gflag), so the loop --
+// unrolled to the maximum rank -- reads every field at a static offset.
 HPTT_HD inline TileOrigin tile_origin(const HpttProblem &P, const HpttTile &T,
                                       uint32_t tile) {
+  (void)P;
   TileOrigin o;
   o.bA = 0;
   o.bB = 0;
   int64_t remX = 0x7fffffff, remY = 0x7fffffff;
   uint32_t rem = tile;
-  const int xc = (T.kind == KIND_ROWS) ? T.wc : T.xc;
-  for (int g = 0; g < T.ng; ++g) {
-    const uint32_t cnt = T.gcnt[g];
-    const uint32_t q = T.gmul[g] ? (umulhi32(rem, T.gmul[g]) >> T.gshr[g]) : rem;
-    const uint32_t c = rem - q * cnt;
-    rem = q;
-    const int d = T.gd[g];
-    const int64_t pos = static_cast<int64_t>(c) * T.gstep[g];
-    o.bA += pos * P.sA[d];
-    o.bB += pos * P.sB[d];
-    if (d == xc) remX = P.n[d] - pos;
-    if (d == T.yc) remY = P.n[d] - pos;
+#ifdef __CUDA_ARCH__
+#pragma unroll
+#endif
+  for (int g = 0; g < HPTT_MAX_RANK; ++g) {
+    if (g < T.ng) {
+      const uint32_t q = T.gmul[g] ? (umulhi32(rem, T.gmul[g]) >> T.gshr[g]) : rem;
+      const uint32_t c = rem - q * T.gcnt[g];
+      rem = q;
+      o.bA += static_cast<int64_t>(c) * T.gsa[g];
+      o.bB += static_cast<int64_t>(c) * T.gsb[g];
+      const int64_t left = T.gn[g] - static_cast<int64_t>(c) * T.gstep[g];
+      if (T.gflag[g] & 1) remX = left;
+      if (T.gflag[g] & 2) remY = left;
+    }
   }
-  o.remX = static_cast<int>(remX);
-  o.remY = static_cast<int>(remY);
+  o.remX = static_cast<int>(remX < 0x7fffffff ? remX : 0x7fffffff);
+  o.remY = static_cast<int>(remY < 0x7fffffff ? remY : 0x7fffffff);
   return o;
 }
 
@@ -173,8 +179,9 @@ HPTT_HD inline HpttThr thread_consts_1d(const HpttProblem &P, const HpttTile &T,
   const int y = tid - qs0 * T.TY;
   h.q0 = q0;
   h.qs0 = qs0;
-  h.inE = static_cast<int64_t>(x) * P.sA[T.xd[0]];
-  h.outE2 = static_cast<int64_t>(y) * P.sB[T.yd[0]];
+  (void)P;
+  h.inE = static_cast<int64_t>(x) * T.sxa;
+  h.outE2 = static_cast<int64_t>(y) * T.syb;
   h.sme = x;
   h.sme2 = y * T.LD;
   h.cxe = T.xc >= 0 ? x : 0;
@@ -189,6 +196,60 @@ HPTT_HD inline int valid_iters(int lim, int q0, uint32_t mul, int shr, int R) {
   return lim > q0 ? fast_div(lim - q0 + R - 1, mul, shr) : 0;
 }
 
+
+// Interior tile of an even single-dim shape (see tile_one).  NJ > 0: both
+// phases run exactly NJ iterations (compile-time trip count); NJ == 0: J1 and
+// J2 at run time.  Offsets fit 32 bits (single-dim sides imply 32-bit
+// tables, i.e. in-tile offsets below 2^31).
+template <typename E, int MODE, bool UPD, int NJ>
+__device__ __forceinline__ void tile_interior(const HpttTile &T, const E *__restrict__ A,
+                                              E *__restrict__ B, const Op<E, MODE, UPD> &op,
+                                              E *sdata, const HpttThr &th, const TileOrigin &o,
+                                              int J1, int J2) {
+  constexpr int J = NJ > 0 ? NJ : hptt_jmax_tile(sizeof(E));
+  const int sYf = static_cast<int>(T.sya);
+  const int sXf = static_cast<int>(T.sxb);
+  const int LD = T.LD, W = T.W, R1 = T.R1, R2 = T.R2, TX = T.TX, TY = T.TY;
+  // run-time trip counts as per-thread slot bounds (q < TY  <=>  j < J1 in
+  // an even tile)
+  (void)J1;
+  (void)J2;
+  const bool ld = th.active & 1, st = th.active & 2;
+  E v[J];
+  const E *src = A + o.bA + th.inE + th.q0 * sYf;
+  const int stepA = R1 * sYf;
+  if (ld) {
+#pragma unroll
+    for (int j = 0; j < J; ++j)
+      if (NJ > 0 || th.q0 + j * R1 < TY) v[j] = __ldg(src + j * stepA);
+  }
+  E *dst = B + o.bB + th.outE2 + th.qs0 * sXf;
+  const int stepB = R2 * sXf;
+  E bv[J];
+  if (UPD && st) {
+#pragma unroll
+    for (int j = 0; j < J; ++j)
+      if (NJ > 0 || th.qs0 + j * R2 < TX) bv[j] = dst[j * stepB];
+  }
+  if (ld) {
+    E *s = sdata + th.q0 * LD + th.sme;
+#pragma unroll
+    for (int j = 0; j < J; ++j)
+      if (NJ > 0 || th.q0 + j * R1 < TY) s[j * R1 * LD] = v[j];
+  }
+  __syncthreads();
+  if (st) {
+    const E *s = sdata + th.sme2 + th.qs0 * W;
+#pragma unroll
+    for (int j = 0; j < J; ++j) {
+      if (NJ > 0 || th.qs0 + j * R2 < TX) {
+        const E a = s[j * R2 * W];
+        const E r = op(a, UPD ? bv[j] : a);
+        if (UPD) dst[j * stepB] = r; else __stcs(dst + j * stepB, r);
+      }
+    }
+  }
+}
 
 // ---------------------------------------------------------------------------
 // One tile through shared memory (one CTA).
@@ -224,55 +285,23 @@ __device__ __forceinline__ void tile_one(const HpttProblem &P, const HpttTile &T
   const TileOrigin o = tile_origin(P, T, tile);
   const int LD = T.LD, W = T.W, R1 = T.R1, R2 = T.R2, J1 = T.J1, J2 = T.J2;
   const int TX = T.TX, TY = T.TY;
+  // Iteration j of a thread covers slot q0 + j*R1 (q0 < R1), so the slot
+  // bound q < TY already implies j < J1: the loops test only the slot bound.
   if (!UPD && LX && LY && T.even && o.remX >= TX && o.remY >= TY) {
     // Interior tile of an even shape: every loading thread has exactly J1
     // rows and every storing thread J2 columns (TY == R1*J1, TX == R2*J2),
-    // so the accesses below -- the same as the general path's -- need no
-    // per-element bounds.  Offsets fit 32 bits (single-dim sides imply
-    // 32-bit tables, i.e. in-tile offsets below 2^31).
-    const int sYf = T.ny == 1 ? static_cast<int>(P.sA[T.yd[0]]) : 0;
-    const int sXf = T.nx == 1 ? static_cast<int>(P.sB[T.xd[0]]) : 0;
-    const bool ld = th.active & 1, st = th.active & 2;
-    E v[J];
-    const E *src = A + o.bA + th.inE + th.q0 * sYf;
-    const int stepA = R1 * sYf;
-    if (ld) {
-#pragma unroll
-      for (int j = 0; j < J; ++j)
-        if (j < J1) v[j] = __ldg(src + j * stepA);
-    }
-    E *dst = B + o.bB + th.outE2 + th.qs0 * sXf;
-    const int stepB = R2 * sXf;
-    E bv[J];
-    if (UPD && st) {
-#pragma unroll
-      for (int j = 0; j < J; ++j)
-        if (j < J2) bv[j] = dst[j * stepB];
-    }
-    if (ld) {
-      E *s = sdata + th.q0 * LD + th.sme;
-#pragma unroll
-      for (int j = 0; j < J; ++j)
-        if (j < J1) s[j * R1 * LD] = v[j];
-    }
-    __syncthreads();
-    if (st) {
-      const E *s = sdata + th.sme2 + th.qs0 * W;
-#pragma unroll
-      for (int j = 0; j < J; ++j) {
-        if (j < J2) {
-          const E a = s[j * R2 * W];
-          const E r = op(a, UPD ? bv[j] : a);
-          if (UPD) dst[j * stepB] = r; else __stcs(dst + j * stepB, r);
-        }
-      }
-    }
+    // so the accesses -- the same as the general path's -- need no
+    // per-element bounds; with J1 == J2 == J not even a trip count.
+    if (J1 == J && J2 == J)
+      tile_interior<E, MODE, UPD, J>(T, A, B, op, sdata, th, o, J, J);
+    else
+      tile_interior<E, MODE, UPD, 0>(T, A, B, op, sdata, th, o, J1, J2);
     return;
   }
   const bool ld_ok = (th.active & 1) && th.cxe < o.remX;
   const bool st_ok = (th.active & 2) && th.cye2 < o.remY;
-  const int sY = (LY && T.ny == 1) ? static_cast<int>(P.sA[T.yd[0]]) : 0;
-  const int sX = (LX && T.nx == 1) ? static_cast<int>(P.sB[T.xd[0]]) : 0;
+  const int sY = LY ? static_cast<int>(T.sya) : 0;
+  const int sX = LX ? static_cast<int>(T.sxb) : 0;
   const int limQY = (LY && T.yc >= 0 && o.remY < TY) ? o.remY : TY;
   const int limQX = (LX && T.xc >= 0 && o.remX < TX) ? o.remX : TX;
   E v[J];
@@ -282,8 +311,8 @@ __device__ __forceinline__ void tile_one(const HpttProblem &P, const HpttTile &T
     for (int j = 0; j < J; ++j) {
       const int q = th.q0 + j * R1;
       if (LY) {
-        if (j < J1 && q < limQY) v[j] = __ldg(src + q * sY);
-      } else if (j < J1 && q < TY) {
+        if (q < limQY) v[j] = __ldg(src + q * sY);
+      } else if (q < TY) {
         const Ent en = tabY[q];
         v[j] = __ldg(src + (en.c < o.remY ? en.off : OffT(0)));
       }
@@ -296,8 +325,8 @@ __device__ __forceinline__ void tile_one(const HpttProblem &P, const HpttTile &T
     for (int j = 0; j < J; ++j) {
       const int q = th.qs0 + j * R2;
       if (LX) {
-        if (j < J2 && q < limQX) bv[j] = dst[q * sX];
-      } else if (j < J2 && q < TX) {
+        if (q < limQX) bv[j] = dst[q * sX];
+      } else if (q < TX) {
         const Ent en = tabX[q];
         bv[j] = dst[en.c < o.remX ? en.off : OffT(0)];
       }
@@ -308,7 +337,7 @@ __device__ __forceinline__ void tile_one(const HpttProblem &P, const HpttTile &T
 #pragma unroll
     for (int j = 0; j < J; ++j) {
       const int q = th.q0 + j * R1;
-      if (j < J1 && q < (LY ? limQY : TY)) s[j * R1 * LD] = v[j];
+      if (q < (LY ? limQY : TY)) s[j * R1 * LD] = v[j];
     }
   }
   __syncthreads();
@@ -320,10 +349,10 @@ __device__ __forceinline__ void tile_one(const HpttProblem &P, const HpttTile &T
     bool ok;
     int64_t off;
     if (LX) {
-      ok = j < J2 && q < limQX;
+      ok = q < limQX;
       off = q * sX;
     } else {
-      ok = j < J2 && q < TX;
+      ok = q < TX;
       Ent en{};
       if (ok) en = tabX[q];
       ok = ok && en.c < o.remX;

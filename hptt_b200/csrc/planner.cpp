@@ -391,7 +391,25 @@ void finish_grid(const HpttProblem &p, HpttTile *t, const int64_t *tile_ext,
 // The fast divisions by R1/R2.  (Tile origins are decoded on the device: a
 // per-tile origin table was measured slower -- every CTA's first loads then
 // wait on a cold read of its own entry.)
-void finish_tables(HpttTile *t) {
+void finish_tables(const HpttProblem &p, HpttTile *t) {
+  // grid levels folded for static-offset reads on the device
+  const int xc = t->kind == KIND_ROWS ? t->wc : t->xc;
+  for (int g = 0; g < HPTT_MAX_RANK; ++g) {
+    if (g < t->ng) {
+      const int d = t->gd[g];
+      t->gsa[g] = static_cast<int64_t>(t->gstep[g]) * p.sA[d];
+      t->gsb[g] = static_cast<int64_t>(t->gstep[g]) * p.sB[d];
+      t->gn[g] = p.n[d];
+      t->gflag[g] = (d == xc ? 1 : 0) | (d == t->yc ? 2 : 0);
+    } else {
+      t->gsa[g] = t->gsb[g] = 0;
+      t->gn[g] = t->gflag[g] = 0;
+    }
+  }
+  t->sxa = t->nx == 1 ? p.sA[t->xd[0]] : 0;
+  t->sxb = t->nx == 1 ? p.sB[t->xd[0]] : 0;
+  t->sya = t->ny == 1 ? p.sA[t->yd[0]] : 0;
+  t->syb = t->ny == 1 ? p.sB[t->yd[0]] : 0;
   fast_div_magic(static_cast<uint32_t>(t->R1 > 0 ? t->R1 : 1), &t->r1_mul, &t->r1_shr);
   fast_div_magic(static_cast<uint32_t>(t->R2 > 0 ? t->R2 : 1), &t->r2_mul, &t->r2_shr);
   fast_div_magic(static_cast<uint32_t>(t->TX > 0 ? t->TX : 1), &t->tx_mul, &t->tx_shr);
@@ -465,7 +483,7 @@ int choose_rows(const HpttProblem &p, const TileParams &tp, HpttTile *t) {
   t->tab2_off = (t->TY * off + 15) & ~15;
   t->thr_off = t->tab2_off + ((t->TY * off + 15) & ~15);
   t->table_bytes = t->thr_off;
-  finish_tables(t);
+  finish_tables(p, t);
   return t->num_tiles ? ST_OK : ST_TOO_LARGE;
 }
 
@@ -621,6 +639,29 @@ int choose_tile(const HpttProblem &p, const TileParams &tp, int update, HpttTile
     }
     tt = cdiv(n, cdiv(n, old));
   }
+  // Whole-extent option (autotuner knob): one side takes its full single-dim
+  // extent, the other shrinks until the tile fits, in whole sectors when it
+  // can.
+  if (tp.full_side && X.d.size() == 1 && Y.d.size() == 1) {
+    Side &F = tp.full_side == 1 ? X : Y;
+    Side &O = tp.full_side == 1 ? Y : X;
+    const int64_t nF = p.n[F.d.back()];
+    if (F.t.back() < nF) {
+      const int64_t oldF = F.t.back(), oldO = O.t.back();
+      F.t.back() = nF;
+      const int64_t sector = std::max<int64_t>(1, 32 / sz);
+      int64_t &to = O.t.back();
+      while (to > 1 && !shape_ok(tp, W, X, Y, sz)) {
+        // largest multiple of a sector below the current extent, else -1
+        const int64_t down = (to - 1) / sector * sector;
+        to = down >= sector ? down : to - 1;
+      }
+      if (!shape_ok(tp, W, X, Y, sz) || to * sz < 32) {
+        F.t.back() = oldF;
+        O.t.back() = oldO;
+      }
+    }
+  }
   // Single-dim sides: round a chunked extent to a multiple of the threads
   // per pass on its side (TY to R1, TX to R2), so every thread of an
   // interior tile has the same iteration count and the kernel's predicate-
@@ -724,7 +765,7 @@ int choose_tile(const HpttProblem &p, const TileParams &tp, int update, HpttTile
   t->tab2_off = a16(t->TY * ent);
   t->thr_off = t->tab2_off + a16(t->TX * ent);
   t->table_bytes = t->thr_off + t->nt * static_cast<int>(sizeof(HpttThr));
-  finish_tables(t);
+  finish_tables(p, t);
   return t->num_tiles ? ST_OK : ST_TOO_LARGE;
 }
 

@@ -42,6 +42,10 @@ struct TileParams {
   int y_first = 0;         // choose the output-side dims before the input side
   int max_iters = 0;       // cap on per-thread iterations of a tile (0: the
                            // kernel's own limit, hptt_jmax_tile)
+  int full_side = 0;       // single-dim tiles: 1 = take the whole X extent,
+                           // 2 = the whole Y extent, shrinking the other side
+                           // (short rows that are not sector-aligned then
+                           // become one contiguous range per tile)
 };
 
 // Reference argument guard (src/hptt.cc:25-56) plus the one check the

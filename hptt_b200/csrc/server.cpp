@@ -63,9 +63,17 @@ struct Request {
 
 // One launch in flight (batched: a stream of the pool; per-call: one request
 // on the shared stream).
+constexpr int kAuxStreams = 3;
+
 struct Launch {
   cudaStream_t stream = nullptr;
   cudaEvent_t done = nullptr;
+  // batched mode: the group kernels of one launch are spread over the
+  // launch's stream and kAuxStreams more (fork/join by events), so groups
+  // overlap on the device instead of running back to back
+  cudaStream_t aux[kAuxStreams] = {};
+  cudaEvent_t fork = nullptr;
+  cudaEvent_t join[kAuxStreams] = {};
   std::vector<Request> reqs;
   bool busy = false;
   // batched mode: device copies of the layout, pinned host staging
@@ -194,8 +202,24 @@ int enqueue_launch(Server *s, Launch *L) {
        cudaMemcpyAsync(L->d_work, L->h_work, lay.work.size() * sizeof(HpttWork),
                        cudaMemcpyHostToDevice, L->stream) != cudaSuccess))
     return ST_CUDA;
-  st = batch_launch_groups(lay.groups, L->d_desc, L->d_work, L->d_counters, L->stream);
-  if (st != ST_OK) return st;
+  if (cudaMemsetAsync(L->d_counters, 0, lay.groups.size() * sizeof(uint32_t), L->stream) !=
+      cudaSuccess)
+    return ST_CUDA;
+  const int naux = static_cast<int>(std::min<size_t>(kAuxStreams, lay.groups.size() - 1));
+  if (naux > 0) {
+    if (cudaEventRecord(L->fork, L->stream) != cudaSuccess) return ST_CUDA;
+    for (int k = 0; k < naux; ++k)
+      if (cudaStreamWaitEvent(L->aux[k], L->fork, 0) != cudaSuccess) return ST_CUDA;
+  }
+  for (size_t gi = 0; gi < lay.groups.size(); ++gi) {
+    cudaStream_t gs = gi % (naux + 1) == 0 ? L->stream : L->aux[gi % (naux + 1) - 1];
+    st = batch_launch_group(lay.groups[gi], L->d_desc, L->d_work, L->d_counters + gi, gs);
+    if (st != ST_OK) return st;
+  }
+  for (int k = 0; k < naux; ++k)
+    if (cudaEventRecord(L->join[k], L->aux[k]) != cudaSuccess ||
+        cudaStreamWaitEvent(L->stream, L->join[k], 0) != cudaSuccess)
+      return ST_CUDA;
   return cudaEventRecord(L->done, L->stream) == cudaSuccess ? ST_OK : ST_CUDA;
 }
 
@@ -353,6 +377,11 @@ void worker_main(Server *s) {
 void free_slots(Server *s) {
   for (Launch &L : s->slots) {
     if (L.done) cudaEventDestroy(L.done);
+    if (L.fork) cudaEventDestroy(L.fork);
+    for (int k = 0; k < kAuxStreams; ++k) {
+      if (L.join[k]) cudaEventDestroy(L.join[k]);
+      if (L.aux[k]) cudaStreamDestroy(L.aux[k]);
+    }
     if (L.stream && L.stream != s->shared_stream) cudaStreamDestroy(L.stream);
     if (L.d_desc) cudaFree(L.d_desc);
     if (L.d_work) cudaFree(L.d_work);
@@ -407,6 +436,14 @@ int hptt_cuda_server_create(const hptt_cuda_serve_config *cfg, hptt_cuda_server_
       st = ST_CUDA;
     if (st == ST_OK && cudaEventCreateWithFlags(&L.done, cudaEventDisableTiming) != cudaSuccess)
       st = ST_CUDA;
+    if (!cfg->per_call) {
+      if (st == ST_OK && cudaEventCreateWithFlags(&L.fork, cudaEventDisableTiming) != cudaSuccess)
+        st = ST_CUDA;
+      for (int k = 0; k < kAuxStreams && st == ST_OK; ++k)
+        if (cudaStreamCreateWithFlags(&L.aux[k], cudaStreamNonBlocking) != cudaSuccess ||
+            cudaEventCreateWithFlags(&L.join[k], cudaEventDisableTiming) != cudaSuccess)
+          st = ST_CUDA;
+    }
   }
   if (st != ST_OK) {
     cudaGetLastError();

@@ -250,12 +250,13 @@ extern "C" int hptt_cuda_debug_check_indexing(int dtype, uint32_t rank, const ui
     s *= L.out_outer[k];
   }
   L.nB = s;
-  // both tile strategies (input side first / output side first), both
-  // update settings, both per-thread iteration limits the tuner tries
-  for (int variant = 0; variant < 8; ++variant) {
+  // every planner knob the tuner tries: side order, both update settings,
+  // both per-thread iteration limits, the whole-extent options
+  for (int variant = 0; variant < 24; ++variant) {
     const int update = variant & 1;
     tp.y_first = (variant >> 1) & 1;
-    tp.max_iters = (variant >> 2) ? hptt_jmax_tile(elem_bytes(P.dtype)) / 2 : 0;
+    tp.max_iters = ((variant >> 2) & 1) ? hptt_jmax_tile(elem_bytes(P.dtype)) / 2 : 0;
+    tp.full_side = variant >> 3;
     HpttTile T;
     st = choose_tile(P, tp, update, &T);
     if (st != ST_OK) return st;
