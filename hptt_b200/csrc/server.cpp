@@ -64,6 +64,7 @@ struct Request {
 // One launch in flight (batched: a stream of the pool; per-call: one request
 // on the shared stream).
 constexpr int kAuxStreams = 3;
+constexpr size_t kForkMinRequests = 32;
 
 struct Launch {
   cudaStream_t stream = nullptr;
@@ -205,7 +206,11 @@ int enqueue_launch(Server *s, Launch *L) {
   if (cudaMemsetAsync(L->d_counters, 0, lay.groups.size() * sizeof(uint32_t), L->stream) !=
       cudaSuccess)
     return ST_CUDA;
-  const int naux = static_cast<int>(std::min<size_t>(kAuxStreams, lay.groups.size() - 1));
+  // fork only launches big enough to gain from overlapping their groups:
+  // each fork costs a few dozen API calls on the scheduler thread
+  const int naux = L->reqs.size() >= kForkMinRequests
+                       ? static_cast<int>(std::min<size_t>(kAuxStreams, lay.groups.size() - 1))
+                       : 0;
   if (naux > 0) {
     if (cudaEventRecord(L->fork, L->stream) != cudaSuccess) return ST_CUDA;
     for (int k = 0; k < naux; ++k)
