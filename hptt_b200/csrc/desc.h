@@ -104,6 +104,9 @@ struct HpttTile {
   // lies wholly inside the tensor every loading thread has exactly J1 rows
   // and every storing thread J2 columns
   int32_t even;
+  // tile extent along the chunked X / Y dim (1 when that side is not
+  // chunked): a tile with remX >= xce and remY >= yce lies wholly inside
+  int32_t xce, yce;
   // fast division by TX and TY: per-thread constants of single-dim tiles
   // with W == 1 are computed from threadIdx instead of read from the table
   uint32_t tx_mul, ty_mul;

@@ -197,57 +197,269 @@ HPTT_HD inline int valid_iters(int lim, int q0, uint32_t mul, int shr, int R) {
 }
 
 
-// Interior tile of an even single-dim shape (see tile_one).  NJ > 0: both
-// phases run exactly NJ iterations (compile-time trip count); NJ == 0: J1 and
-// J2 at run time.  Offsets fit 32 bits (single-dim sides imply 32-bit
-// tables, i.e. in-tile offsets below 2^31).
-template <typename E, int MODE, bool UPD, int NJ>
+// Interior tile of an even single-dim shape (see tile_one): every loading
+// thread has exactly J1 rows and every storing thread J2 columns.  Each phase
+// runs with a compile-time trip count (N == J1 or J2, chosen by a chain of
+// uniform compares once per phase): run-time bounds inside the unrolled loops
+// compiled to a branch per access.  Offsets fit 32 bits (single-dim sides
+// imply 32-bit tables, i.e. in-tile offsets below 2^31).
+template <typename E, int N>
+__device__ __forceinline__ void interior_load(const E *__restrict__ src, int stepA, E *s,
+                                              int sstep) {
+  E v[N];
+#pragma unroll
+  for (int j = 0; j < N; ++j) v[j] = __ldg(src + j * stepA);
+#pragma unroll
+  for (int j = 0; j < N; ++j) s[j * sstep] = v[j];
+}
+
+template <typename E, int MODE, bool UPD, int N>
+__device__ __forceinline__ void interior_store(const E *s, int sstep, E *__restrict__ dst,
+                                               int stepB, const Op<E, MODE, UPD> &op) {
+#pragma unroll
+  for (int j = 0; j < N; ++j) {
+    const E a = s[j * sstep];
+    __stcs(dst + j * stepB, op(a, a));
+  }
+}
+
+template <typename E, int N>
+__device__ __forceinline__ void interior_load_n(int n, const E *__restrict__ src, int stepA,
+                                                E *s, int sstep) {
+  if (n == N) {
+    interior_load<E, N>(src, stepA, s, sstep);
+  } else if constexpr (N > 1) {
+    interior_load_n<E, N - 1>(n, src, stepA, s, sstep);
+  }
+}
+
+template <typename E, int MODE, bool UPD, int N>
+__device__ __forceinline__ void interior_store_n(int n, const E *s, int sstep,
+                                                 E *__restrict__ dst, int stepB,
+                                                 const Op<E, MODE, UPD> &op) {
+  if (n == N) {
+    interior_store<E, MODE, UPD, N>(s, sstep, dst, stepB, op);
+  } else if constexpr (N > 1) {
+    interior_store_n<E, MODE, UPD, N - 1>(n, s, sstep, dst, stepB, op);
+  }
+}
+
+template <typename E, int MODE, bool UPD>
 __device__ __forceinline__ void tile_interior(const HpttTile &T, const E *__restrict__ A,
                                               E *__restrict__ B, const Op<E, MODE, UPD> &op,
                                               E *sdata, const HpttThr &th, const TileOrigin &o,
                                               int J1, int J2) {
-  constexpr int J = NJ > 0 ? NJ : hptt_jmax_tile(sizeof(E));
+  constexpr int J = hptt_jmax_tile(sizeof(E));
   const int sYf = static_cast<int>(T.sya);
   const int sXf = static_cast<int>(T.sxb);
-  const int LD = T.LD, W = T.W, R1 = T.R1, R2 = T.R2, TX = T.TX, TY = T.TY;
-  // run-time trip counts as per-thread slot bounds (q < TY  <=>  j < J1 in
-  // an even tile)
-  (void)J1;
-  (void)J2;
+  const int LD = T.LD, W = T.W, R1 = T.R1, R2 = T.R2;
+  if (th.active & 1)
+    interior_load_n<E, J>(J1, A + o.bA + th.inE + th.q0 * sYf, R1 * sYf,
+                          sdata + th.q0 * LD + th.sme, R1 * LD);
+  __syncthreads();
+  if (th.active & 2)
+    interior_store_n<E, MODE, UPD, J>(J2, sdata + th.sme2 + th.qs0 * W, R2 * W,
+                                      B + o.bB + th.outE2 + th.qs0 * sXf, R2 * sXf, op);
+}
+
+// Edge or uneven tile of a single-dim copy/scale shape: the same compile-
+// time loops as the interior, with every slot index clamped to the last
+// valid row (column).  An iteration past the edge repeats that slot: it
+// reads the same element again and writes the same value to the same place
+// (a row slot in shared memory, a column of B), which changes nothing --
+// so no per-element branch is needed.  Threads whose own element lies
+// outside the tile skip their phase.
+template <typename E, int N>
+__device__ __forceinline__ void clamped_load(const E *__restrict__ src, int sY, int q0, int R1,
+                                             int lim, E *s, int LD) {
+  E v[N];
+#pragma unroll
+  for (int j = 0; j < N; ++j) v[j] = __ldg(src + min(q0 + j * R1, lim - 1) * sY);
+#pragma unroll
+  for (int j = 0; j < N; ++j) s[min(q0 + j * R1, lim - 1) * LD] = v[j];
+}
+
+template <typename E, int MODE, bool UPD, int N>
+__device__ __forceinline__ void clamped_store(const E *s, int W, int qs0, int R2, int lim,
+                                              E *__restrict__ dst, int sX,
+                                              const Op<E, MODE, UPD> &op) {
+#pragma unroll
+  for (int j = 0; j < N; ++j) {
+    const int q = min(qs0 + j * R2, lim - 1);
+    const E a = s[q * W];
+    __stcs(dst + q * sX, op(a, a));
+  }
+}
+
+template <typename E, int N>
+__device__ __forceinline__ void clamped_load_n(int n, const E *__restrict__ src, int sY, int q0,
+                                               int R1, int lim, E *s, int LD) {
+  if (n == N) {
+    clamped_load<E, N>(src, sY, q0, R1, lim, s, LD);
+  } else if constexpr (N > 1) {
+    clamped_load_n<E, N - 1>(n, src, sY, q0, R1, lim, s, LD);
+  }
+}
+
+template <typename E, int MODE, bool UPD, int N>
+__device__ __forceinline__ void clamped_store_n(int n, const E *s, int W, int qs0, int R2,
+                                                int lim, E *__restrict__ dst, int sX,
+                                                const Op<E, MODE, UPD> &op) {
+  if (n == N) {
+    clamped_store<E, MODE, UPD, N>(s, W, qs0, R2, lim, dst, sX, op);
+  } else if constexpr (N > 1) {
+    clamped_store_n<E, MODE, UPD, N - 1>(n, s, W, qs0, R2, lim, dst, sX, op);
+  }
+}
+
+template <typename E, int MODE, bool UPD>
+__device__ __forceinline__ void tile_clamped(const HpttTile &T, const E *__restrict__ A,
+                                             E *__restrict__ B, const Op<E, MODE, UPD> &op,
+                                             E *sdata, const HpttThr &th, const TileOrigin &o) {
+  constexpr int J = hptt_jmax_tile(sizeof(E));
+  const int TX = T.TX, TY = T.TY;
+  const int limR = (T.yc >= 0 && o.remY < TY) ? o.remY : TY;
+  const int limC = (T.xc >= 0 && o.remX < TX) ? o.remX : TX;
+  if ((th.active & 1) && th.cxe < o.remX)
+    clamped_load_n<E, J>(T.J1, A + o.bA + th.inE, static_cast<int>(T.sya), th.q0, T.R1, limR,
+                         sdata + th.sme, T.LD);
+  __syncthreads();
+  if ((th.active & 2) && th.cye2 < o.remY)
+    clamped_store_n<E, MODE, UPD, J>(T.J2, sdata + th.sme2, T.W, th.qs0, T.R2, limC,
+                                     B + o.bB + th.outE2, static_cast<int>(T.sxb), op);
+}
+
+// Single-dim tiles that also read B, shapes with J1 == J2 == J: one
+// compile-time instance (the B values must live across the barrier, so the
+// two phases cannot be dispatched separately).
+// Interior tile of an even shape: no bounds at all.
+template <typename E, int MODE, bool UPD>
+__device__ __forceinline__ void tile_interior_upd(const HpttTile &T, const E *__restrict__ A,
+                                                  E *__restrict__ B, const Op<E, MODE, UPD> &op,
+                                                  E *sdata, const HpttThr &th,
+                                                  const TileOrigin &o) {
+  constexpr int J = hptt_jmax_tile(sizeof(E));
+  const int sYf = static_cast<int>(T.sya);
+  const int sXf = static_cast<int>(T.sxb);
+  const int LD = T.LD, W = T.W, R1 = T.R1, R2 = T.R2;
   const bool ld = th.active & 1, st = th.active & 2;
-  E v[J];
   const E *src = A + o.bA + th.inE + th.q0 * sYf;
-  const int stepA = R1 * sYf;
+  E *dst = B + o.bB + th.outE2 + th.qs0 * sXf;
+  const int stepA = R1 * sYf, stepB = R2 * sXf;
+  E v[J], bv[J];
   if (ld) {
 #pragma unroll
-    for (int j = 0; j < J; ++j)
-      if (NJ > 0 || th.q0 + j * R1 < TY) v[j] = __ldg(src + j * stepA);
+    for (int j = 0; j < J; ++j) v[j] = __ldg(src + j * stepA);
   }
-  E *dst = B + o.bB + th.outE2 + th.qs0 * sXf;
-  const int stepB = R2 * sXf;
-  E bv[J];
-  if (UPD && st) {
+  if (st) {
 #pragma unroll
-    for (int j = 0; j < J; ++j)
-      if (NJ > 0 || th.qs0 + j * R2 < TX) bv[j] = dst[j * stepB];
+    for (int j = 0; j < J; ++j) bv[j] = dst[j * stepB];
   }
   if (ld) {
     E *s = sdata + th.q0 * LD + th.sme;
 #pragma unroll
-    for (int j = 0; j < J; ++j)
-      if (NJ > 0 || th.q0 + j * R1 < TY) s[j * R1 * LD] = v[j];
+    for (int j = 0; j < J; ++j) s[j * R1 * LD] = v[j];
   }
   __syncthreads();
   if (st) {
     const E *s = sdata + th.sme2 + th.qs0 * W;
 #pragma unroll
+    for (int j = 0; j < J; ++j) dst[j * stepB] = op(s[j * R2 * W], bv[j]);
+  }
+}
+
+// Edge tile: slot indices clamped as in tile_clamped; every B value is read
+// before the barrier, so a repeated column computes and writes the same
+// value again.  (Used for 8- and 16-byte elements: with 4-byte elements' 16
+// iterations it needs too many registers, and their edge tiles take the
+// general path.)
+template <typename E, int MODE, bool UPD>
+__device__ __forceinline__ void tile_full_upd(const HpttTile &T, const E *__restrict__ A,
+                                              E *__restrict__ B, const Op<E, MODE, UPD> &op,
+                                              E *sdata, const HpttThr &th,
+                                              const TileOrigin &o) {
+  constexpr int J = hptt_jmax_tile(sizeof(E));
+  const int sY = static_cast<int>(T.sya);
+  const int sX = static_cast<int>(T.sxb);
+  const int LD = T.LD, W = T.W, R1 = T.R1, R2 = T.R2;
+  const int limR = T.yc >= 0 && o.remY < T.TY ? o.remY : T.TY;
+  const int limC = T.xc >= 0 && o.remX < T.TX ? o.remX : T.TX;
+  const bool ld = (th.active & 1) && th.cxe < o.remX;
+  const bool st = (th.active & 2) && th.cye2 < o.remY;
+  const E *src = A + o.bA + th.inE;
+  E *dst = B + o.bB + th.outE2;
+  E v[J], bv[J];
+  if (ld) {
+#pragma unroll
+    for (int j = 0; j < J; ++j) v[j] = __ldg(src + min(th.q0 + j * R1, limR - 1) * sY);
+  }
+  if (st) {
+#pragma unroll
+    for (int j = 0; j < J; ++j) bv[j] = dst[min(th.qs0 + j * R2, limC - 1) * sX];
+  }
+  if (ld) {
+#pragma unroll
+    for (int j = 0; j < J; ++j) sdata[min(th.q0 + j * R1, limR - 1) * LD + th.sme] = v[j];
+  }
+  __syncthreads();
+  if (st) {
+#pragma unroll
     for (int j = 0; j < J; ++j) {
-      if (NJ > 0 || th.qs0 + j * R2 < TX) {
-        const E a = s[j * R2 * W];
-        const E r = op(a, UPD ? bv[j] : a);
-        if (UPD) dst[j * stepB] = r; else __stcs(dst + j * stepB, r);
-      }
+      const int q = min(th.qs0 + j * R2, limC - 1);
+      dst[q * sX] = op(sdata[th.sme2 + q * W], bv[j]);
     }
+  }
+}
+
+// Interior tile of a table-driven copy/scale shape (a side with several
+// dims): every chunk coordinate is inside the tensor, so the table offsets
+// need no checks.  Compile-time trip counts per phase; slots past TY (TX) in
+// an uneven shape are clamped to the last one and repeat it (same element,
+// same value).
+template <typename E, typename OffT, int N>
+__device__ __forceinline__ void table_load(const E *__restrict__ src,
+                                           const HpttTabEnt<OffT> *__restrict__ tabY, int q0,
+                                           int R1, int TY, E *s, int LD) {
+  E v[N];
+#pragma unroll
+  for (int j = 0; j < N; ++j) v[j] = __ldg(src + tabY[min(q0 + j * R1, TY - 1)].off);
+#pragma unroll
+  for (int j = 0; j < N; ++j) s[min(q0 + j * R1, TY - 1) * LD] = v[j];
+}
+
+template <typename E, int MODE, bool UPD, typename OffT, int N>
+__device__ __forceinline__ void table_store(const E *s, int W,
+                                            const HpttTabEnt<OffT> *__restrict__ tabX, int qs0,
+                                            int R2, int TX, E *__restrict__ dst,
+                                            const Op<E, MODE, UPD> &op) {
+#pragma unroll
+  for (int j = 0; j < N; ++j) {
+    const int q = min(qs0 + j * R2, TX - 1);
+    const E a = s[q * W];
+    __stcs(dst + tabX[q].off, op(a, a));
+  }
+}
+
+template <typename E, typename OffT, int N>
+__device__ __forceinline__ void table_load_n(int n, const E *__restrict__ src,
+                                             const HpttTabEnt<OffT> *__restrict__ tabY, int q0,
+                                             int R1, int TY, E *s, int LD) {
+  if (n == N) {
+    table_load<E, OffT, N>(src, tabY, q0, R1, TY, s, LD);
+  } else if constexpr (N > 1) {
+    table_load_n<E, OffT, N - 1>(n, src, tabY, q0, R1, TY, s, LD);
+  }
+}
+
+template <typename E, int MODE, bool UPD, typename OffT, int N>
+__device__ __forceinline__ void table_store_n(int n, const E *s, int W,
+                                              const HpttTabEnt<OffT> *__restrict__ tabX, int qs0,
+                                              int R2, int TX, E *__restrict__ dst,
+                                              const Op<E, MODE, UPD> &op) {
+  if (n == N) {
+    table_store<E, MODE, UPD, OffT, N>(s, W, tabX, qs0, R2, TX, dst, op);
+  } else if constexpr (N > 1) {
+    table_store_n<E, MODE, UPD, OffT, N - 1>(n, s, W, tabX, qs0, R2, TX, dst, op);
   }
 }
 
@@ -287,15 +499,39 @@ __device__ __forceinline__ void tile_one(const HpttProblem &P, const HpttTile &T
   const int TX = T.TX, TY = T.TY;
   // Iteration j of a thread covers slot q0 + j*R1 (q0 < R1), so the slot
   // bound q < TY already implies j < J1: the loops test only the slot bound.
+  if (UPD && LX && LY && J1 == J && J2 == J) {
+    // (the clamped edge form needs too many registers with 4-byte
+    // elements' 16 iterations; their edge tiles take the general path)
+    if (T.even && o.remX >= TX && o.remY >= TY) {
+      tile_interior_upd<E, MODE, UPD>(T, A, B, op, sdata, th, o);
+      return;
+    }
+    if constexpr (sizeof(E) > 4) {
+      tile_full_upd<E, MODE, UPD>(T, A, B, op, sdata, th, o);
+      return;
+    }
+  }
   if (!UPD && LX && LY && T.even && o.remX >= TX && o.remY >= TY) {
     // Interior tile of an even shape: every loading thread has exactly J1
     // rows and every storing thread J2 columns (TY == R1*J1, TX == R2*J2),
     // so the accesses -- the same as the general path's -- need no
-    // per-element bounds; with J1 == J2 == J not even a trip count.
-    if (J1 == J && J2 == J)
-      tile_interior<E, MODE, UPD, J>(T, A, B, op, sdata, th, o, J, J);
-    else
-      tile_interior<E, MODE, UPD, 0>(T, A, B, op, sdata, th, o, J1, J2);
+    // per-element bounds.
+    tile_interior<E, MODE, UPD>(T, A, B, op, sdata, th, o, J1, J2);
+    return;
+  }
+  if (!UPD && LX && LY) {
+    tile_clamped<E, MODE, UPD>(T, A, B, op, sdata, th, o);
+    return;
+  }
+  if (!UPD && !(LX && LY) && o.remX >= T.xce && o.remY >= T.yce) {
+    // interior tile of a table-driven shape
+    if (th.active & 1)
+      table_load_n<E, OffT, J>(J1, A + o.bA + th.inE, tabY, th.q0, R1, TY,
+                               sdata + th.sme, LD);
+    __syncthreads();
+    if (th.active & 2)
+      table_store_n<E, MODE, UPD, OffT, J>(J2, sdata + th.sme2, W, tabX, th.qs0, R2, TX,
+                                           B + o.bB + th.outE2, op);
     return;
   }
   const bool ld_ok = (th.active & 1) && th.cxe < o.remX;

@@ -406,6 +406,12 @@ void finish_tables(const HpttProblem &p, HpttTile *t) {
       t->gn[g] = t->gflag[g] = 0;
     }
   }
+  t->xce = 1;
+  t->yce = 1;
+  for (int i = 0; i < t->nx; ++i)
+    if (t->xd[i] == t->xc) t->xce = t->xt[i];
+  for (int i = 0; i < t->ny; ++i)
+    if (t->yd[i] == t->yc) t->yce = t->yt[i];
   t->sxa = t->nx == 1 ? p.sA[t->xd[0]] : 0;
   t->sxb = t->nx == 1 ? p.sB[t->xd[0]] : 0;
   t->sya = t->ny == 1 ? p.sA[t->yd[0]] : 0;

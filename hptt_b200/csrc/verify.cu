@@ -107,11 +107,75 @@ int replay_tile(const HpttProblem &P, const HpttTile &T, int update, const Layou
   // the kernel indexes single-dim sides as q * stride in 32-bit ints
   if (ly && T.ny == 1 && T.TY > 1 && P.sA[T.yd[0]] > 0x7fffffffLL) return 128;
   if (lx && T.nx == 1 && T.TX > 1 && P.sB[T.xd[0]] > 0x7fffffffLL) return 129;
+  // tiles with single-dim sides run compile-time loops (copy/scale tiles
+  // always, update tiles of 8/16-byte elements when J1 == J2 == J): interior
+  // tiles of even shapes
+  // unclamped, every other tile with slot indices clamped to the last valid
+  // row/column (kernels.cuh: tile_clamped, tile_full_upd), so an iteration
+  // past the edge repeats a slot with the same element
+  const bool clamped_kind =
+      lx && ly && (!update || (T.J1 == J && T.J2 == J && elem_bytes(P.dtype) > 4));
+  // copy/scale tiles with a multi-dim side: interior tiles run the same
+  // compile-time loops over the tables (kernels.cuh: table_load/store), slots
+  // past TY (TX) clamped to the last one
+  const bool table_kind = !update && !(lx && ly);
+  const bool tracks = clamped_kind || table_kind;
+  std::vector<int64_t> writer(tracks ? static_cast<size_t>(L.nB) : 0, -1);
+  std::vector<uint32_t> writer_tile(tracks ? static_cast<size_t>(L.nB) : 0, 0);
   for (uint32_t tile = 0; tile < T.num_tiles; ++tile) {
     const TileOrigin o = tile_origin(P, T, tile);
     std::fill(slot.begin(), slot.end(), -1);
     const int limQY = (ly && T.yc >= 0 && o.remY < T.TY) ? o.remY : T.TY;
     const int limQX = (lx && T.xc >= 0 && o.remX < T.TX) ? o.remX : T.TX;
+    const bool interior = T.even && o.remX >= T.TX && o.remY >= T.TY;
+    const bool table_interior = table_kind && o.remX >= T.xce && o.remY >= T.yce;
+    if ((clamped_kind && !interior) || table_interior) {
+      const int limR = table_interior ? T.TY : (T.yc >= 0 && o.remY < T.TY) ? o.remY : T.TY;
+      const int limC = table_interior ? T.TX : (T.xc >= 0 && o.remX < T.TX) ? o.remX : T.TX;
+      if (limR < 1 || limC < 1) return 140;
+      for (int t = 0; t < T.nt; ++t) {
+        const HpttThr &th = thr[t];
+        if (!((th.active & 1) && th.cxe < o.remX)) continue;
+        for (int j = 0; j < T.J1; ++j) {
+          const int q = std::min(th.q0 + j * T.R1, limR - 1);
+          if (q < 0 || q >= T.TY) return 141;
+          if (!(tabY[q].c < o.remY)) return 142;
+          const int64_t si = static_cast<int64_t>(q) * T.LD + th.sme;
+          if (si < 0 || si >= smem_elems) return 143;
+          const int64_t ia = o.bA + th.inE + static_cast<int64_t>(tabY[q].off);
+          if (ia < 0 || ia >= L.nA) return 144;
+          // a repeated slot must hold the same element
+          if (slot[si] >= 0 && slot[si] != ia) return 145;
+          slot[si] = ia;
+        }
+      }
+      for (int t = 0; t < T.nt; ++t) {
+        const HpttThr &th = thr[t];
+        if (!((th.active & 2) && th.cye2 < o.remY)) continue;
+        for (int j = 0; j < T.J2; ++j) {
+          const int q = std::min(th.qs0 + j * T.R2, limC - 1);
+          if (q < 0 || q >= T.TX) return 146;
+          if (!(tabX[q].c < o.remX)) return 147;
+          const int64_t si = static_cast<int64_t>(th.sme2) + static_cast<int64_t>(q) * T.W;
+          if (si < 0 || si >= smem_elems) return 148;
+          const int64_t ia = slot[si];
+          if (ia < 0) return 149;  // reads a slot no load wrote
+          const int64_t ib = o.bB + th.outE2 + static_cast<int64_t>(tabX[q].off);
+          if (ib < 0 || ib >= L.nB) return 150;
+          if (map_a_to_b(L, ia) != ib) return 151;
+          // a repeated write must come from the same tile with the same element
+          if (writer[ib] >= 0 && (writer[ib] != ia || writer_tile[ib] != tile)) return 152;
+          if (writer[ib] < 0) {
+            if (writes[ib] != 0) return 153;  // written by another tile
+            writer[ib] = ia;
+            writer_tile[ib] = tile;
+            writes[ib] = 1;
+            ++*checked;
+          }
+        }
+      }
+      continue;
+    }
     // load phase: iteration j of a thread loads row slot q0 + j*R1 when
     // j < J1 and the slot is inside the tile (single-dim Y side: inside the
     // tensor too); a table slot outside the tensor re-reads element 0
