@@ -40,11 +40,12 @@ constexpr int vmax_rows() {
   return sizeof(E) == 4 ? 4 : (sizeof(E) == 8 ? 2 : 1);
 }
 
-// Resident-CTA targets: one step below k_tile's, since the persistent loop
-// keeps its own state live across the tile body.
+// Resident-CTA targets: 3 (80 registers) for every tile body -- the
+// persistent loop keeps its own state live across the body, and the tile
+// bodies' compile-time paths need the room; rows bodies are not bounded.
 template <bool UPD, int SHAPE>
 constexpr int min_ctas() {
-  return SHAPE >= 3 ? 1 : (UPD ? 3 : 4);
+  return SHAPE >= 3 ? 1 : 3;
 }
 
 // Persistent kernel of one group: CTAs take items [begin, end) of the work
@@ -83,11 +84,11 @@ __global__ void __launch_bounds__(kNT, (min_ctas<UPD, SHAPE>()))
         if (k) __syncthreads();
         E *s = reinterpret_cast<E *>(smem);
         if (SHAPE == 0)
-          tile_one<E, MODE, UPD, uint32_t, false, false>(a.p, a.t, A, B, tab, op, s, tile);
+          tile_one<E, MODE, UPD, uint32_t, false, false, false>(a.p, a.t, A, B, tab, op, s, tile);
         else if (SHAPE == 1)
-          tile_one<E, MODE, UPD, uint32_t, true, true>(a.p, a.t, A, B, tab, op, s, tile);
+          tile_one<E, MODE, UPD, uint32_t, true, true, false>(a.p, a.t, A, B, tab, op, s, tile);
         else
-          tile_one<E, MODE, UPD, int64_t, false, false>(a.p, a.t, A, B, tab, op, s, tile);
+          tile_one<E, MODE, UPD, int64_t, false, false, false>(a.p, a.t, A, B, tab, op, s, tile);
       } else if (SHAPE == 3) {
         rows_one<E, MODE, UPD, uint32_t, vmax_rows<E>()>(a.p, a.t, A, B, tab, op, tile);
       } else if (SHAPE == 4) {

@@ -480,7 +480,9 @@ __device__ __forceinline__ void table_store_n(int n, const E *s, int W,
 // table read (the tables hold exactly these values; the CPU replay checks
 // that).
 // ---------------------------------------------------------------------------
-template <typename E, int MODE, bool UPD, typename OffT, bool LX, bool LY>
+// UPD_FAST: update tiles may take the bounds-free and clamped forms (more
+// registers: kernels that also keep persistent-loop state turn it off).
+template <typename E, int MODE, bool UPD, typename OffT, bool LX, bool LY, bool UPD_FAST = true>
 __device__ __forceinline__ void tile_one(const HpttProblem &P, const HpttTile &T,
                                          const E *__restrict__ A, E *__restrict__ B,
                                          const unsigned char *__restrict__ tables,
@@ -499,7 +501,7 @@ __device__ __forceinline__ void tile_one(const HpttProblem &P, const HpttTile &T
   const int TX = T.TX, TY = T.TY;
   // Iteration j of a thread covers slot q0 + j*R1 (q0 < R1), so the slot
   // bound q < TY already implies j < J1: the loops test only the slot bound.
-  if (UPD && LX && LY && J1 == J && J2 == J) {
+  if (UPD && UPD_FAST && LX && LY && J1 == J && J2 == J) {
     // (the clamped edge form needs too many registers with 4-byte
     // elements' 16 iterations; their edge tiles take the general path)
     if (T.even && o.remX >= TX && o.remY >= TY) {
