@@ -258,7 +258,9 @@ def run_ours(args, rank, world, dist):
     roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak,
                 "unit": "GB/s", "frac": round(achieved / peak, 4),
                 "traffic": traffic, "kernel": "k_tile" if dom == "tile" else "k_rows",
-                "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs, burst copy)",
+                "peak_source": ("measured (MEASURED_PEAKS.json hbm_gbs, burst copy)"
+                                if peak_kind == "measured" else
+                                "fallback 6650 GB/s (MEASURED_PEAKS.json absent)"),
                 "launches": dom_launches,
                 "algorithmic_bytes_per_launch": int(dom_bytes // max(1, dom_launches)),
                 "share_of_device_time": round(dom_ms / device_ms, 4)}
@@ -274,6 +276,9 @@ def run_ours(args, rank, world, dist):
         if not args.no_served:
             served = run_served(args, pool)
         del pool, pool_buffers
+    contraction = None
+    if world == 1 and args.case is None and not args.no_contraction:
+        contraction = run_contractions(args)
     gpu_launches = sum(p.launches for p, _, _, _ in plans) * args.steps
 
     cpu = None
@@ -298,6 +303,7 @@ def run_ours(args, rank, world, dist):
         "cpu_baseline": cpu,
         "batched": batched,
         "served": served,
+        "contraction": contraction,
         "kernel_ms_per_step": round(device_ms / args.steps, 4),
     }
     return out
@@ -512,6 +518,111 @@ def run_served(args, plans):
     return out
 
 
+def run_contractions(args):
+    """Tensor contractions through the transposes (hptt_cuda_contract_*):
+    seeded synthetic TTGT workloads (workloads.contraction_cases), each timed
+    three ways on the same device buffers with CUDA events:
+      ours       one contraction exec (graph replay: operand transposes, one
+                 strided-batched cuBLAS GEMM, output transpose with alpha/beta)
+      gemm_only  a contraction of the same m, n, k, batch whose operands and
+                 output already have GEMM layouts (no transposes): the floor
+                 the transposes add to
+      torch      torch.einsum on the same buffers plus the alpha/beta update
+                 (its own permute copies and GEMM), full f32 (no TF32)."""
+    import torch
+    import hptt_b200 as h
+    from hptt_b200 import workloads as w
+
+    torch.backends.cuda.matmul.allow_tf32 = False
+    cases = w.contraction_cases()
+    g = torch.Generator(device="cuda").manual_seed(99)
+    stream = torch.cuda.current_stream()
+    sptr = stream.cuda_stream
+
+    def rnd(n, dt):
+        t = _tdtype(torch, dt)
+        if dt in ("c64", "c128"):
+            rt = torch.float32 if dt == "c64" else torch.float64
+            return torch.view_as_complex(torch.rand(n, 2, generator=g, device="cuda",
+                                                    dtype=rt) * 2 - 1)
+        return torch.rand(n, generator=g, device="cuda", dtype=t) * 2 - 1
+
+    def timed(fn, reps=args.contract_reps):
+        for _ in range(3):
+            fn()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(reps):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+    rows = []
+    tot = {"flops": 0, "ours": 0.0, "gemm": 0.0, "torch": 0.0}
+    for c in cases:
+        dt = c["dtype"]
+        na, nb, nc = (int(np.prod(c[k])) for k in ("size_a", "size_b", "size_c"))
+        A, B, C = rnd(na, dt), rnd(nb, dt), rnd(nc, dt)
+        plan = h.create_contraction(A, B, C, c["size_a"], c["labels_a"], c["size_b"],
+                                    c["labels_b"], c["labels_c"], c["alpha"], c["beta"],
+                                    dtype=dt)
+        info = plan.info()
+        ours = timed(lambda: plan.exec_on(sptr))
+        info = plan.info()
+        # the same GEMM with every tensor already in GEMM layout
+        m, n, k, bt = info["m"], info["n"], info["k"], info["batch"]
+        A2, B2, C2 = rnd(m * k * bt, dt), rnd(k * n * bt, dt), rnd(m * n * bt, dt)
+        gplan = h.create_contraction(A2, B2, C2, [m, k, bt], "mkb", [k, n, bt], "knb", "mnb",
+                                     c["alpha"], c["beta"], dtype=dt)
+        assert gplan.info()["transposes"] == 0
+        gemm = timed(lambda: gplan.exec_on(sptr))
+        # torch.einsum on the same column-major buffers: reversed dims, row-major views
+        sa, sb, sc = ("".join(reversed(c[k])) for k in ("labels_a", "labels_b", "labels_c"))
+        Av = A.view(list(reversed(c["size_a"])))
+        Bv = B.view(list(reversed(c["size_b"])))
+        Cv = C.view(list(reversed(c["size_c"])))
+        al, be = c["alpha"], c["beta"]
+
+        def torch_step():
+            r = torch.einsum(f"{sa},{sb}->{sc}", Av, Bv)
+            if be != 0.0:
+                Cv.mul_(be).add_(r, alpha=al)
+            else:
+                Cv.copy_(r.mul_(al) if al != 1.0 else r)
+        tms = timed(torch_step)
+        fl = info["flops"]
+        rows.append({"dtype": dt, "spec": f"{''.join(c['labels_a'])},{''.join(c['labels_b'])}"
+                                          f"->{''.join(c['labels_c'])}",
+                     "size_a": c["size_a"], "size_b": c["size_b"],
+                     "m": m, "n": n, "k": k, "batch": bt, "transposes": info["transposes"],
+                     "transpose_bytes": info["transpose_bytes"],
+                     "ms": round(ours, 4), "gemm_only_ms": round(gemm, 4),
+                     "torch_einsum_ms": round(tms, 4),
+                     "tflops": round(fl / ours / 1e9, 2),
+                     "transpose_share": round(max(0.0, 1 - gemm / ours), 4),
+                     "speedup_vs_torch": round(tms / ours, 3)})
+        tot["flops"] += fl
+        tot["ours"] += ours
+        tot["gemm"] += gemm
+        tot["torch"] += tms
+        plan.destroy()
+        gplan.destroy()
+        del A, B, C, A2, B2, C2
+    return {"workload": f"{len(cases)} seeded synthetic contractions (f32/f64, one c64, one "
+                        "c128; 1-3 M/N/K labels, 0-1 batch label, random label orders; "
+                        "GEMM m, n ~ 1-4 K, k ~ 0.5-2 K)",
+            "api": "hptt_cuda_contract_exec_on (CUDA graph replay)",
+            "total_ms": round(tot["ours"], 4), "gemm_only_ms": round(tot["gemm"], 4),
+            "torch_einsum_ms": round(tot["torch"], 4),
+            "tflops": round(tot["flops"] / tot["ours"] / 1e9, 2),
+            "transpose_share": round(max(0.0, 1 - tot["gemm"] / tot["ours"]), 4),
+            "speedup_vs_torch_einsum": round(tot["torch"] / tot["ours"], 3),
+            "reps": args.contract_reps, "cases": rows}
+
+
 # --------------------------------------------------------------------------
 # CPU reference
 # --------------------------------------------------------------------------
@@ -650,6 +761,9 @@ def main():
     ap.add_argument("--serve-seconds", type=float, default=2.0,
                     help="arrival window per rate (60 for the full served workload)")
     ap.add_argument("--batch-reps", type=int, default=10)
+    ap.add_argument("--no-contraction", action="store_true",
+                    help="skip the tensor-contraction (transpose-GEMM-transpose) section")
+    ap.add_argument("--contract-reps", type=int, default=20)
     ap.add_argument("--case", type=int, default=None,
                     help="run only transpose I of the workload (profiling)")
     args = ap.parse_args()

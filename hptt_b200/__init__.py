@@ -42,6 +42,7 @@ STATUS = {
     4: "bad size value", 5: "bad permutation", 6: "bad dtype", 7: "CUDA error",
     8: "no CUDA device", 9: "allocation failed", 10: "memory budget exceeded",
     11: "invalid handle", 12: "timeout", 13: "too large", 14: "busy",
+    15: "labels do not describe a contraction", 16: "cuBLAS error",
 }
 # argument errors for which the reference returns nullptr
 _NULLPTR_STATUSES = {1, 2, 3, 4, 5}
@@ -56,6 +57,7 @@ class HpttError(RuntimeError):
 _lib = None
 _u32p = ctypes.POINTER(ctypes.c_uint32)
 _dp = ctypes.POINTER(ctypes.c_double)
+_i32p = ctypes.POINTER(ctypes.c_int32)
 
 
 def library_path() -> str:
@@ -77,6 +79,17 @@ class ServeStats(ctypes.Structure):
                [(n, ctypes.c_double) for n in (
                     "elapsed_s", "throughput_rps", "gbs", "mean_batch", "lat_mean_us",
                     "lat_p50_us", "lat_p99_us", "lat_p999_us", "lat_max_us")]
+
+    def as_dict(self):
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
+class ContractStats(ctypes.Structure):
+    """hptt_cuda_contract_stats (include/hptt_cuda.h)."""
+    _fields_ = [("m", ctypes.c_uint64), ("n", ctypes.c_uint64), ("k", ctypes.c_uint64),
+                ("batch", ctypes.c_uint64), ("flops", ctypes.c_uint64),
+                ("transpose_bytes", ctypes.c_uint64), ("workspace_bytes", ctypes.c_uint64),
+                ("transposes", ctypes.c_uint32), ("graph", ctypes.c_uint32)]
 
     def as_dict(self):
         return {name: getattr(self, name) for name, _ in self._fields_}
@@ -129,6 +142,22 @@ def load_library() -> ctypes.CDLL:
                                                  ctypes.c_uint64, c_dbl,
                                                  ctypes.POINTER(ServeStats)]),
         "hptt_cuda_server_destroy": (c_int, [c_vp]),
+        "hptt_cuda_contract_create": (c_int, [c_int, c_u32, _u32p, _i32p, c_u32, _u32p, _i32p,
+                                              c_u32, _i32p, _dp, _dp, c_int, c_vp, c_vp, c_vp,
+                                              c_vp, ctypes.c_uint64, ctypes.POINTER(c_vp)]),
+        "hptt_cuda_contract_inspect": (c_int, [c_int, c_u32, _u32p, _i32p, c_u32, _u32p, _i32p,
+                                               c_u32, _i32p, ctypes.c_char_p, c_sz,
+                                               ctypes.POINTER(ctypes.c_uint64)]),
+        "hptt_cuda_contract_exec": (c_int, [c_vp]),
+        "hptt_cuda_contract_exec_on": (c_int, [c_vp, c_vp]),
+        "hptt_cuda_contract_reset_data": (c_int, [c_vp, c_vp, c_vp, c_vp]),
+        "hptt_cuda_contract_set_coef": (c_int, [c_vp, _dp, _dp, c_int]),
+        "hptt_cuda_contract_set_stream": (c_int, [c_vp, c_vp]),
+        "hptt_cuda_contract_set_graph": (c_int, [c_vp, c_int]),
+        "hptt_cuda_contract_sync": (c_int, [c_vp]),
+        "hptt_cuda_contract_info": (c_int, [c_vp, ctypes.POINTER(ContractStats)]),
+        "hptt_cuda_contract_describe": (c_int, [c_vp, ctypes.c_char_p, c_sz]),
+        "hptt_cuda_contract_destroy": (c_int, [c_vp]),
         "hptt_cuda_tune_cache_load": (c_int, [ctypes.c_char_p]),
         "hptt_cuda_tune_cache_save": (c_int, [ctypes.c_char_p]),
         "hptt_cuda_tune_cache_clear": (c_int, []),
@@ -469,6 +498,158 @@ class TransServer:
             self.destroy()
         except Exception:
             pass
+
+
+# --------------------------------------------------------------------------
+# Tensor contraction through the transposes (hptt_cuda_contract_*)
+# --------------------------------------------------------------------------
+def _i32(v: Sequence[int]):
+    return (ctypes.c_int32 * max(1, len(v)))(*[int(x) for x in v])
+
+
+def _label_codes(*lists):
+    """Map arbitrary hashable labels (characters, ints) to int32 codes."""
+    codes = {}
+    out = []
+    for lst in lists:
+        out.append([codes.setdefault(x, len(codes)) for x in lst])
+    return out
+
+
+def parse_spec(spec: str):
+    """'acid,dbcj->abij' -> (labels_a, labels_b, labels_c), one character per
+    dimension, fastest (stride-1) dimension first."""
+    lhs, arrow, rhs = spec.replace(" ", "").partition("->")
+    ops = lhs.split(",")
+    if not arrow or len(ops) != 2:
+        raise ValueError(f"contraction spec needs the form 'ab,bc->ac': {spec!r}")
+    return list(ops[0]), list(ops[1]), list(rhs)
+
+
+class Contraction:
+    """C[lc] = alpha * sum_K A[la] * B[lb] + beta * C[lc] on the device:
+    transposes (this library's kernels), one strided-batched cuBLAS GEMM and
+    an output transpose that applies alpha and beta."""
+
+    def __init__(self, handle: int, dtype: int, keep=()):
+        self._h = ctypes.c_void_p(handle)
+        self.dtype = dtype
+        self._keep = keep
+
+    def exec(self) -> None:
+        self._check(load_library().hptt_cuda_contract_exec(self._h), "exec")
+
+    def __call__(self) -> None:
+        self.exec()
+
+    def exec_on(self, stream) -> None:
+        self._check(load_library().hptt_cuda_contract_exec_on(self._h, _stream_ptr(stream)),
+                    "exec_on")
+
+    def reset_data(self, A, B, C) -> None:
+        self._keep = (A, B, C) + tuple(self._keep[3:])
+        self._check(load_library().hptt_cuda_contract_reset_data(
+            self._h, _device_ptr(A), _device_ptr(B), _device_ptr(C)), "reset_data")
+
+    def set_coef(self, alpha, beta, complex_scalars: Optional[bool] = None) -> None:
+        if complex_scalars is None:
+            complex_scalars = isinstance(alpha, complex) or isinstance(beta, complex)
+        self._check(load_library().hptt_cuda_contract_set_coef(
+            self._h, _scalar(alpha), _scalar(beta), int(bool(complex_scalars))), "set_coef")
+
+    def set_stream(self, stream) -> None:
+        self._check(load_library().hptt_cuda_contract_set_stream(self._h, _stream_ptr(stream)),
+                    "set_stream")
+
+    def set_graph(self, on: bool) -> None:
+        self._check(load_library().hptt_cuda_contract_set_graph(self._h, int(bool(on))),
+                    "set_graph")
+
+    def sync(self) -> None:
+        self._check(load_library().hptt_cuda_contract_sync(self._h), "sync")
+
+    def info(self) -> dict:
+        st = ContractStats()
+        self._check(load_library().hptt_cuda_contract_info(self._h, ctypes.byref(st)), "info")
+        return st.as_dict()
+
+    def describe(self) -> str:
+        buf = ctypes.create_string_buffer(4096)
+        self._check(load_library().hptt_cuda_contract_describe(self._h, buf, 4096), "describe")
+        return buf.value.decode()
+
+    def destroy(self) -> None:
+        if self._h.value:
+            load_library().hptt_cuda_contract_destroy(self._h)
+            self._h = ctypes.c_void_p(0)
+
+    def __del__(self):
+        try:
+            self.destroy()
+        except Exception:
+            pass
+
+    @staticmethod
+    def _check(st: int, what: str) -> None:
+        if st != 0:
+            raise HpttError(st, "contraction " + what)
+
+
+def inspect_contraction(dtype, size_a: Sequence[int], labels_a, size_b: Sequence[int],
+                        labels_b, labels_c):
+    """Host-only: the layout the contraction would use and its workspace
+    bytes (no device, no data)."""
+    la, lb, lc = _label_codes(labels_a, labels_b, labels_c)
+    lib = load_library()
+    buf = ctypes.create_string_buffer(4096)
+    ws = ctypes.c_uint64(0)
+    st = lib.hptt_cuda_contract_inspect(dtype_code(dtype), len(la), _u32(size_a), _i32(la),
+                                        len(lb), _u32(size_b), _i32(lb), len(lc), _i32(lc),
+                                        buf, 4096, ctypes.byref(ws))
+    if st != 0:
+        raise HpttError(st, "inspect_contraction")
+    return buf.value.decode(), ws.value
+
+
+def create_contraction(A, B, C, size_a: Sequence[int], labels_a, size_b: Sequence[int],
+                       labels_b, labels_c, alpha=1.0, beta=0.0, dtype=None,
+                       complex_scalars: Optional[bool] = None, workspace=None,
+                       workspace_bytes: int = 0, use_graph: bool = True) -> Contraction:
+    """Plan C[labels_c] = alpha * sum A[labels_a] * B[labels_b] + beta * C.
+
+    Sizes are column-major extents (stride-1 dimension first); labels are
+    any hashable values (one per dimension).  ``workspace`` (a device buffer
+    of at least ``inspect_contraction(...)[1]`` bytes) avoids the plan's own
+    allocation."""
+    code = dtype_code(dtype if dtype is not None else A)
+    la, lb, lc = _label_codes(labels_a, labels_b, labels_c)
+    if complex_scalars is None:
+        complex_scalars = code in (C64, C128) and (
+            isinstance(alpha, complex) or isinstance(beta, complex))
+    lib = load_library()
+    h = ctypes.c_void_p(0)
+    ws_ptr = _device_ptr(workspace) if workspace is not None else None
+    if workspace is not None and not workspace_bytes:
+        workspace_bytes = int(workspace.numel() * workspace.element_size())
+    st = lib.hptt_cuda_contract_create(
+        code, len(la), _u32(size_a), _i32(la), len(lb), _u32(size_b), _i32(lb), len(lc),
+        _i32(lc), _scalar(alpha), _scalar(beta), int(bool(complex_scalars)),
+        _device_ptr(A), _device_ptr(B), _device_ptr(C), ws_ptr, int(workspace_bytes),
+        ctypes.byref(h))
+    if st != 0:
+        raise HpttError(st, "create_contraction")
+    c = Contraction(h.value, code, keep=(A, B, C, workspace))
+    if not use_graph:
+        c.set_graph(False)
+    return c
+
+
+def contract(spec: str, A, B, C, size_a: Sequence[int], size_b: Sequence[int],
+             alpha=1.0, beta=0.0, **kw) -> Contraction:
+    """``create_contraction`` from an index string, e.g. ``'acid,dbcj->abij'``
+    (one character per dimension, stride-1 dimension first)."""
+    la, lb, lc = parse_spec(spec)
+    return create_contraction(A, B, C, size_a, la, size_b, lb, lc, alpha, beta, **kw)
 
 
 def tune_cache_load(path: Optional[str] = None) -> None:

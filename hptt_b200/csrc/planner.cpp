@@ -37,6 +37,8 @@ const char *status_string(int st) {
     case ST_TIMEOUT: return "bounded wait ran out";
     case ST_TOO_LARGE: return "size beyond what this build supports";
     case ST_BUSY: return "no free slot";
+    case ST_LABELS: return "contraction labels do not describe a contraction";
+    case ST_BLAS: return "cuBLAS call failed";
     default: return "unknown status";
   }
 }

@@ -26,6 +26,8 @@ enum Status : int {
   ST_TIMEOUT = 12,         // a bounded wait ran out
   ST_TOO_LARGE = 13,       // a size beyond what this build supports
   ST_BUSY = 14,            // no free slot (served form)
+  ST_LABELS = 15,          // contraction labels do not describe a contraction
+  ST_BLAS = 16,            // a cuBLAS call failed (contraction GEMM)
 };
 
 const char *status_string(int st);

@@ -8,6 +8,9 @@ benchmarks and the full-size tests.  No data: callers fill tensors.
                   rescale: a rank-2 f32 tensor of 200 MB needs ~7071 per dim)
 * hard_cases()    c64/c128 rank 6, stride-1 extents 2-16, ~256 MB per tensor
 * batch_cases()   4096 mixed transposes, 4 KB - 16 MB each (~6 GB in total)
+* contraction_cases()  tensor contractions for the transpose-GEMM-transpose
+                  path: 1-3 M, N and K labels, 0-1 batch labels, random label
+                  orders in every tensor, GEMM extents m, n ~ 1-4 K, k ~ 0.5-2 K
 """
 from __future__ import annotations
 
@@ -89,6 +92,52 @@ def batch_cases(count: int = 4096, seed: int = 7, lo_bytes: float = 4096,
             alpha, beta = float(rng.uniform(-2, 2)), float(rng.uniform(-2, 2))
         cases.append({"dtype": dtype, "in_size": size, "perm": perm,
                       "alpha": alpha, "beta": beta})
+    return cases
+
+
+def _split(rng, total: float, parts: int) -> List[int]:
+    """Extents of `parts` labels whose product is about `total`."""
+    if parts == 0:
+        return []
+    w = rng.uniform(0.5, 1.5, parts)
+    ext = [max(2, int(round(total ** (x / w.sum())))) for x in w]
+    return ext
+
+
+def contraction_cases(count: int = 8, seed: int = 11) -> List[Dict]:
+    """Seeded synthetic contractions C[lc] = alpha * A[la] B[lb] + beta * C:
+    f32 and f64 (one c64 and one c128), label orders drawn at random, so most
+    operands need a transpose before the GEMM and most outputs one after."""
+    rng = np.random.default_rng(seed)
+    names = ["f32", "f64", "f32", "f64", "f32", "f64", "c64", "c128"]
+    letters = "abcdefghijklmnop"
+    cases = []
+    for i in range(count):
+        dtype = names[i % len(names)]
+        cplx = dtype in ("c64", "c128")
+        nm, nn, nk = (int(rng.integers(1, 4)) for _ in range(3))
+        nb = int(rng.integers(0, 2))
+        lab = iter(letters)
+        M = [next(lab) for _ in range(nm)]
+        N = [next(lab) for _ in range(nn)]
+        K = [next(lab) for _ in range(nk)]
+        Bt = [next(lab) for _ in range(nb)]
+        scale = 0.5 if cplx else 1.0
+        m = math.exp(rng.uniform(math.log(1024), math.log(4096))) * scale
+        n = math.exp(rng.uniform(math.log(1024), math.log(4096))) * scale
+        k = math.exp(rng.uniform(math.log(512), math.log(2048))) * scale
+        bsz = 4 if nb else 1
+        ext = dict(zip(M, _split(rng, m / bsz ** 0.5, nm)))
+        ext.update(zip(N, _split(rng, n / bsz ** 0.5, nn)))
+        ext.update(zip(K, _split(rng, k, nk)))
+        ext.update(zip(Bt, [bsz] * nb))
+        la = [str(x) for x in rng.permutation(M + K + Bt)]
+        lb = [str(x) for x in rng.permutation(K + N + Bt)]
+        lc = [str(x) for x in rng.permutation(M + N + Bt)]
+        alpha, beta = (1.0, 0.0) if i % 2 == 0 else (0.5, -1.5)
+        cases.append({"dtype": dtype, "labels_a": la, "labels_b": lb, "labels_c": lc,
+                      "size_a": [ext[x] for x in la], "size_b": [ext[x] for x in lb],
+                      "size_c": [ext[x] for x in lc], "alpha": alpha, "beta": beta})
     return cases
 
 

@@ -51,7 +51,9 @@ enum hptt_cuda_status {
   HPTT_ERR_HANDLE = 11,
   HPTT_ERR_TIMEOUT = 12,
   HPTT_ERR_TOO_LARGE = 13,
-  HPTT_ERR_BUSY = 14
+  HPTT_ERR_BUSY = 14,
+  HPTT_ERR_LABELS = 15,
+  HPTT_ERR_BLAS = 16
 };
 
 typedef struct hptt_cuda_plan_s *hptt_cuda_plan_t;
@@ -296,6 +298,77 @@ int hptt_cuda_server_run_poisson(hptt_cuda_server_t server, const hptt_cuda_plan
                                  uint64_t seed, double drain_timeout_s,
                                  hptt_cuda_serve_stats *stats);
 int hptt_cuda_server_destroy(hptt_cuda_server_t server);
+
+/*
+ * Tensor contraction through this library's transposes (TTGT):
+ *
+ *     C[labels_c] = alpha * sum_K A[labels_a] * B[labels_b] + beta * C[labels_c]
+ *
+ * No counterpart in the reference, which only transposes: this wraps its
+ * plan usage (create_plan, exec, reset_data; README.md:48-72) around a GEMM
+ * the way transpose-based contraction code calls it.  Tensors are dense and column-major like the transposes'
+ * (sizes listed fastest dimension first); labels are arbitrary int32 values,
+ * each at most once per tensor.  A label in A and C is an M index, in B and C
+ * an N index, in A and B (not C) a summed K index, in all three a batch
+ * index; C's extents come from A and B.  Not contractions (HPTT_ERR_LABELS):
+ * a label of one operand alone that C lacks, a C label in neither operand,
+ * a shared label with two extents.
+ *
+ * exec runs: A -> A-hat and B -> B-hat transposes (alpha = 1, beta = 0; each
+ * skipped when the operand already has a GEMM layout), one strided-batched
+ * cuBLAS GEMM into C-hat, and the output transpose C = alpha * C-hat(perm) +
+ * beta * C, which reads C only when |beta| >= 1e-16 (the transposes' rule,
+ * inc/hptt/impl/hptt_trans_impl.h:75-78).  When C-hat already has C's
+ * layout the GEMM applies alpha and beta itself.  Label orders and layouts
+ * are chosen to transpose the fewest elements.  f32 GEMMs run in full f32
+ * (no reduced-precision tensor-core modes).  From the second exec on, the
+ * whole sequence replays as one CUDA graph (transposes of A and B in
+ * parallel branches) unless hptt_cuda_contract_set_graph(plan, 0).
+ *
+ *   rank_a, rank_b  1..8;  rank_c 0..8 (0: C is one element)
+ *   alpha, beta     two doubles each, as for hptt_cuda_plan_create
+ *   A, B, C         device pointers; never freed by the plan
+ *   workspace       device memory for A-hat, B-hat, C-hat and the GEMM
+ *                   library's workspace, 256-byte aligned, at least the
+ *                   bytes hptt_cuda_contract_inspect reports
+ *                   (HPTT_ERR_BUDGET otherwise); NULL: the plan allocates
+ *                   and frees its own.
+ */
+typedef struct hptt_cuda_contract_s *hptt_cuda_contract_t;
+typedef struct {
+  uint64_t m, n, k, batch;    /* GEMM extents */
+  uint64_t flops;             /* 2 m n k batch (8 m n k batch for complex) */
+  uint64_t transpose_bytes;   /* bytes the transposes move per exec */
+  uint64_t workspace_bytes;
+  uint32_t transposes;        /* transposes per exec, 0..3 */
+  uint32_t graph;             /* 1 once exec replays a captured graph */
+} hptt_cuda_contract_stats;
+int hptt_cuda_contract_create(int dtype, uint32_t rank_a, const uint32_t *size_a,
+                              const int32_t *labels_a, uint32_t rank_b, const uint32_t *size_b,
+                              const int32_t *labels_b, uint32_t rank_c,
+                              const int32_t *labels_c, const double *alpha,
+                              const double *beta, int complex_scalars, const void *A,
+                              const void *B, void *C, void *workspace,
+                              uint64_t workspace_bytes, hptt_cuda_contract_t *plan);
+/* Host-only: validate, choose the layout, write its summary and the
+ * workspace size (no device needed). */
+int hptt_cuda_contract_inspect(int dtype, uint32_t rank_a, const uint32_t *size_a,
+                               const int32_t *labels_a, uint32_t rank_b,
+                               const uint32_t *size_b, const int32_t *labels_b,
+                               uint32_t rank_c, const int32_t *labels_c, char *buf, size_t len,
+                               uint64_t *workspace_bytes);
+int hptt_cuda_contract_exec(hptt_cuda_contract_t plan);
+int hptt_cuda_contract_exec_on(hptt_cuda_contract_t plan, void *stream);
+int hptt_cuda_contract_reset_data(hptt_cuda_contract_t plan, const void *A, const void *B,
+                                  void *C);
+int hptt_cuda_contract_set_coef(hptt_cuda_contract_t plan, const double *alpha,
+                                const double *beta, int complex_scalars);
+int hptt_cuda_contract_set_stream(hptt_cuda_contract_t plan, void *stream);
+int hptt_cuda_contract_set_graph(hptt_cuda_contract_t plan, int use_graph);
+int hptt_cuda_contract_sync(hptt_cuda_contract_t plan);
+int hptt_cuda_contract_info(hptt_cuda_contract_t plan, hptt_cuda_contract_stats *info);
+int hptt_cuda_contract_describe(hptt_cuda_contract_t plan, char *buf, size_t len);
+int hptt_cuda_contract_destroy(hptt_cuda_contract_t plan);
 
 /* Autotune cache: the tile parameters the tuner picked, one entry per
  * (GPU name, dtype, fused rank, fused perm, size class, B read).  Plans

@@ -14,8 +14,10 @@
 // Exit status 0 when every check passes.
 #include <cuda_runtime.h>
 #include <dlfcn.h>
+#include <hptt/contraction.h>
 #include <hptt/hptt.h>
 
+#include <cmath>
 #include <complex>
 #include <cstdio>
 #include <cstring>
@@ -89,6 +91,18 @@ int run_guard() {
   check(hptt::create_plan<float>(in, out, size, perm, 1.0f, 0.0f, 1, 0.0, {}, {6, 4}) ==
             nullptr,
         "out_outer length");
+  // contraction (include/hptt/contraction.h): invalid labels fail before any
+  // device work
+  float dummy_c[1] = {0.0f};
+  check(hptt::create_contraction<float>(in, {3, 4}, {'i', 'k'}, in, {5, 2}, {'k', 'j'}, dummy_c,
+                                        {'i', 'j'}, 1.0f, 0.0f) == nullptr,
+        "contraction: K extents differ");
+  check(hptt::create_contraction<float>(in, {3, 4}, {'i', 'k'}, in, {4, 2}, {'k', 'j'}, dummy_c,
+                                        {'i'}, 1.0f, 0.0f) == nullptr,
+        "contraction: j summed over B alone");
+  check(hptt::create_contraction<float>(in, {3, 3}, {'i', 'i'}, in, {3}, {'i'}, dummy_c, {'i'},
+                                        1.0f, 0.0f) == nullptr,
+        "contraction: repeated label");
   // factories: same guard, raw pointer result
   check(create_trans_plan_impl_s(in, out, 1, {4}, {0}, 1.0f, 0.0f, 1, 0.0, {}, {}) == nullptr,
         "factory rank 1");
@@ -233,6 +247,69 @@ void gpu_factory(void *lib, const char *sym, std::mt19937_64 &rng) {
               rng);
 }
 
+// C[a,b,i,j] = alpha * sum_{c,d} A[a,c,i,d] B[d,b,c,j] + beta * C through
+// hptt::create_contraction, against a plain loop within the dot-product
+// error bound (K + 6) u sum |a||b| + |beta c| terms.
+void gpu_contraction(std::mt19937_64 &rng) {
+  const uint32_t na = 6, nc = 5, ni = 7, nd = 4, nb = 9, nj = 3;
+  const std::vector<uint32_t> sa{na, nc, ni, nd}, sb{nd, nb, nc, nj};
+  const size_t NA = na * nc * ni * nd, NB = nd * nb * nc * nj, NC = na * nb * ni * nj;
+  std::uniform_real_distribution<double> u(-1.0, 1.0);
+  std::vector<double> a(NA), b(NB), c0(NC), got(NC);
+  for (auto &x : a) x = u(rng);
+  for (auto &x : b) x = u(rng);
+  for (auto &x : c0) x = u(rng);
+  double *da = nullptr, *db = nullptr, *dc = nullptr;
+  cudaMalloc(&da, NA * 8);
+  cudaMalloc(&db, NB * 8);
+  cudaMalloc(&dc, NC * 8);
+  cudaMemcpy(da, a.data(), NA * 8, cudaMemcpyHostToDevice);
+  cudaMemcpy(db, b.data(), NB * 8, cudaMemcpyHostToDevice);
+  cudaMemcpy(dc, c0.data(), NC * 8, cudaMemcpyHostToDevice);
+  const double alpha = 0.5, beta = -1.25;
+  auto plan = hptt::create_contraction<double>(da, sa, {'a', 'c', 'i', 'd'}, db, sb,
+                                               {'d', 'b', 'c', 'j'}, dc,
+                                               {'a', 'b', 'i', 'j'}, alpha, beta);
+  check(plan != nullptr, "create_contraction f64");
+  if (plan) {
+    check(plan->exec() == HPTT_OK && plan->exec() == HPTT_OK, "contraction exec twice");
+    check(plan->sync() == HPTT_OK, "contraction sync");
+    cudaMemcpy(got.data(), dc, NC * 8, cudaMemcpyDeviceToHost);
+    int bad = 0;
+    std::vector<double> want = c0;
+    for (int rep = 0; rep < 2; ++rep) {
+      std::vector<double> next(NC);
+      for (uint32_t A_ = 0; A_ < na; ++A_)
+        for (uint32_t B_ = 0; B_ < nb; ++B_)
+          for (uint32_t I = 0; I < ni; ++I)
+            for (uint32_t J = 0; J < nj; ++J) {
+              double s = 0, sabs = 0;
+              for (uint32_t C_ = 0; C_ < nc; ++C_)
+                for (uint32_t D = 0; D < nd; ++D) {
+                  const double x = a[A_ + na * (C_ + nc * (I + ni * D))];
+                  const double y = b[D + nd * (B_ + nb * (C_ + nc * J))];
+                  s += x * y;
+                  sabs += std::fabs(x * y);
+                }
+              const size_t o = A_ + na * (B_ + nb * (I + ni * J));
+              next[o] = alpha * s + beta * want[o];
+              if (rep == 1) {
+                const double tol = 2 * (nc * nd + 6) * 1.2e-16 *
+                                   (std::fabs(alpha) * sabs + std::fabs(beta * want[o])) *
+                                   4.0;
+                if (!(std::fabs(got[o] - next[o]) <= tol + 1e-300)) ++bad;
+              }
+            }
+      want = next;
+    }
+    check(bad == 0, "contraction f64 within the error bound (" + std::to_string(bad) + " bad)");
+  }
+  plan.reset();
+  cudaFree(da);
+  cudaFree(db);
+  cudaFree(dc);
+}
+
 int run_gpu(const char *libpath) {
   std::mt19937_64 rng(0);
   gpu_type<float>("f32", rng);
@@ -240,6 +317,7 @@ int run_gpu(const char *libpath) {
   gpu_type<hptt::FloatComplex>("c64", rng);
   gpu_type<hptt::DoubleComplex>("c128", rng);
   gpu_reset_data(rng);
+  gpu_contraction(rng);
   {
     // complex scalars (extension)
     const std::vector<uint32_t> size{8, 6, 4, 5}, perm{3, 1, 0, 2};

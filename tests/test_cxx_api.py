@@ -45,7 +45,7 @@ def cxx_binary(tmp_path_factory):
     cmd = [os.environ.get("CXX", "g++"), "-std=c++14", "-O1", "-Wall",
            "-I", os.path.join(ROOT, "include"), "-I", ORACLE_DIR,
            "-I", os.path.join(CUDA, "include"), SRC, "-o", out,
-           "-L", PKG, "-lhptt", "-L", ORACLE_DIR, "-loracle",
+           "-L", PKG, "-lhptt", "-lhptt_cuda", "-L", ORACLE_DIR, "-loracle",
            "-L", os.path.join(CUDA, "lib64"), "-lcudart", "-ldl",
            f"-Wl,-rpath,{PKG}:{ORACLE_DIR}:{os.path.join(CUDA, 'lib64')}"]
     r = subprocess.run(cmd, capture_output=True, text=True)
