@@ -411,55 +411,86 @@ __device__ __forceinline__ void tile_full_upd(const HpttTile &T, const E *__rest
   }
 }
 
-// Interior tile of a table-driven copy/scale shape (a side with several
-// dims): every chunk coordinate is inside the tensor, so the table offsets
-// need no checks.  Compile-time trip counts per phase; slots past TY (TX) in
-// an uneven shape are clamped to the last one and repeat it (same element,
-// same value).
-template <typename E, typename OffT, int N>
-__device__ __forceinline__ void table_load(const E *__restrict__ src,
-                                           const HpttTabEnt<OffT> *__restrict__ tabY, int q0,
-                                           int R1, int TY, E *s, int LD) {
-  E v[N];
-#pragma unroll
-  for (int j = 0; j < N; ++j) v[j] = __ldg(src + tabY[min(q0 + j * R1, TY - 1)].off);
-#pragma unroll
-  for (int j = 0; j < N; ++j) s[min(q0 + j * R1, TY - 1) * LD] = v[j];
-}
+// Run f with a compile-time trip count equal to n (1 <= n <= N): a chain of
+// uniform compares, once per phase.
+template <int N>
+struct TripCount {
+  static constexpr int value = N;
+};
 
-template <typename E, int MODE, bool UPD, typename OffT, int N>
-__device__ __forceinline__ void table_store(const E *s, int W,
-                                            const HpttTabEnt<OffT> *__restrict__ tabX, int qs0,
-                                            int R2, int TX, E *__restrict__ dst,
-                                            const Op<E, MODE, UPD> &op) {
-#pragma unroll
-  for (int j = 0; j < N; ++j) {
-    const int q = min(qs0 + j * R2, TX - 1);
-    const E a = s[q * W];
-    __stcs(dst + tabX[q].off, op(a, a));
+template <int N, typename F>
+__device__ __forceinline__ void with_trip_count(int n, F &&f) {
+  if (n == N) {
+    f(TripCount<N>());
+  } else if constexpr (N > 1) {
+    with_trip_count<N - 1>(n, f);
   }
 }
 
-template <typename E, typename OffT, int N>
-__device__ __forceinline__ void table_load_n(int n, const E *__restrict__ src,
-                                             const HpttTabEnt<OffT> *__restrict__ tabY, int q0,
-                                             int R1, int TY, E *s, int LD) {
-  if (n == N) {
-    table_load<E, OffT, N>(src, tabY, q0, R1, TY, s, LD);
-  } else if constexpr (N > 1) {
-    table_load_n<E, OffT, N - 1>(n, src, tabY, q0, R1, TY, s, LD);
+// Interior tile of a table-driven shape (a side with several dims, or the
+// 64-bit-offset kernel): every chunk coordinate is inside the tensor, so no
+// offset needs a check.  Compile-time trip counts per phase; slots past TY
+// (TX) in an uneven shape are clamped to the last one and repeat it (same
+// element, same value).  A single-dim side takes q * stride instead of its
+// table entry (the tables hold exactly that).  Update tiles read their B
+// values before the barrier, at the same clamped slots as the stores: a
+// repeated slot recomputes the same value from the same original B element,
+// since every B read of the tile precedes every B write.
+template <typename E, int MODE, bool UPD, typename OffT, bool LX, bool LY>
+__device__ __forceinline__ void tile_table_interior(const HpttTile &T, const E *__restrict__ A,
+                                                    E *__restrict__ B,
+                                                    const HpttTabEnt<OffT> *__restrict__ tabY,
+                                                    const HpttTabEnt<OffT> *__restrict__ tabX,
+                                                    const Op<E, MODE, UPD> &op, E *sdata,
+                                                    const HpttThr &th, const TileOrigin &o) {
+  constexpr int J = hptt_jmax_tile(sizeof(E));
+  const int LD = T.LD, W = T.W, R1 = T.R1, R2 = T.R2, TX = T.TX, TY = T.TY;
+  const int sY = LY ? static_cast<int>(T.sya) : 0;
+  const int sX = LX ? static_cast<int>(T.sxb) : 0;
+  const E *src = A + o.bA + th.inE;
+  E *dst = B + o.bB + th.outE2;
+  const bool ld = th.active & 1, st = th.active & 2;
+  E bv[UPD ? J : 1];
+  if (UPD && st) {
+    with_trip_count<J>(T.J2, [&](auto n) {
+      constexpr int N = decltype(n)::value;
+#pragma unroll
+      for (int j = 0; j < N; ++j) {
+        const int q = min(th.qs0 + j * R2, TX - 1);
+        bv[UPD ? j : 0] = dst[LX ? static_cast<OffT>(q * sX) : tabX[q].off];
+      }
+    });
   }
-}
-
-template <typename E, int MODE, bool UPD, typename OffT, int N>
-__device__ __forceinline__ void table_store_n(int n, const E *s, int W,
-                                              const HpttTabEnt<OffT> *__restrict__ tabX, int qs0,
-                                              int R2, int TX, E *__restrict__ dst,
-                                              const Op<E, MODE, UPD> &op) {
-  if (n == N) {
-    table_store<E, MODE, UPD, OffT, N>(s, W, tabX, qs0, R2, TX, dst, op);
-  } else if constexpr (N > 1) {
-    table_store_n<E, MODE, UPD, OffT, N - 1>(n, s, W, tabX, qs0, R2, TX, dst, op);
+  if (ld) {
+    with_trip_count<J>(T.J1, [&](auto n) {
+      constexpr int N = decltype(n)::value;
+      E v[N];
+#pragma unroll
+      for (int j = 0; j < N; ++j) {
+        const int q = min(th.q0 + j * R1, TY - 1);
+        v[j] = __ldg(src + (LY ? static_cast<OffT>(q * sY) : tabY[q].off));
+      }
+      E *s = sdata + th.sme;
+#pragma unroll
+      for (int j = 0; j < N; ++j) s[min(th.q0 + j * R1, TY - 1) * LD] = v[j];
+    });
+  }
+  __syncthreads();
+  if (st) {
+    with_trip_count<J>(T.J2, [&](auto n) {
+      constexpr int N = decltype(n)::value;
+      const E *s = sdata + th.sme2;
+#pragma unroll
+      for (int j = 0; j < N; ++j) {
+        const int q = min(th.qs0 + j * R2, TX - 1);
+        const E a = s[q * W];
+        E *d = dst + (LX ? static_cast<OffT>(q * sX) : tabX[q].off);
+        if (UPD)
+          *d = op(a, bv[UPD ? j : 0]);
+        else
+          __stcs(d, op(a, a));
+      }
+    });
   }
 }
 
@@ -525,15 +556,8 @@ __device__ __forceinline__ void tile_one(const HpttProblem &P, const HpttTile &T
     tile_clamped<E, MODE, UPD>(T, A, B, op, sdata, th, o);
     return;
   }
-  if (!UPD && !(LX && LY) && o.remX >= T.xce && o.remY >= T.yce) {
-    // interior tile of a table-driven shape
-    if (th.active & 1)
-      table_load_n<E, OffT, J>(J1, A + o.bA + th.inE, tabY, th.q0, R1, TY,
-                               sdata + th.sme, LD);
-    __syncthreads();
-    if (th.active & 2)
-      table_store_n<E, MODE, UPD, OffT, J>(J2, sdata + th.sme2, W, tabX, th.qs0, R2, TX,
-                                           B + o.bB + th.outE2, op);
+  if ((!UPD || UPD_FAST) && !(LX && LY) && o.remX >= T.xce && o.remY >= T.yce) {
+    tile_table_interior<E, MODE, UPD, OffT, LX, LY>(T, A, B, tabY, tabX, op, sdata, th, o);
     return;
   }
   const bool ld_ok = (th.active & 1) && th.cxe < o.remX;

@@ -115,10 +115,11 @@ int replay_tile(const HpttProblem &P, const HpttTile &T, int update, const Layou
   // past the edge repeats a slot with the same element
   const bool clamped_kind =
       lx && ly && (!update || (T.J1 == J && T.J2 == J && elem_bytes(P.dtype) > 4));
-  // copy/scale tiles with a multi-dim side: interior tiles run the same
-  // compile-time loops over the tables (kernels.cuh: table_load/store), slots
-  // past TY (TX) clamped to the last one
-  const bool table_kind = !update && !(lx && ly);
+  // tiles with a multi-dim side (copy, scale and update): interior tiles run
+  // compile-time loops over the tables (kernels.cuh: tile_table_interior),
+  // slots past TY (TX) clamped to the last one; update tiles read B at the
+  // store slots before the barrier
+  const bool table_kind = !(lx && ly);
   const bool tracks = clamped_kind || table_kind;
   std::vector<int64_t> writer(tracks ? static_cast<size_t>(L.nB) : 0, -1);
   std::vector<uint32_t> writer_tile(tracks ? static_cast<size_t>(L.nB) : 0, 0);
