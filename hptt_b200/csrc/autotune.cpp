@@ -38,8 +38,8 @@ std::string gpu_name() {
 const char *env_path() { return std::getenv("HPTT_B200_TUNE_CACHE"); }
 
 // Cache file: one line per key,
-// "key|run vmin smem rows_min y_first iters full_side"
-// (missing trailing fields read as 0).
+// "key|run vmin smem rows_min y_first iters full_side walk"
+// (missing trailing fields read as 0, walk as 1).
 void read_cache_stream(std::istream &f) {
   std::string line;
   while (std::getline(f, line)) {
@@ -51,6 +51,7 @@ void read_cache_stream(std::istream &f) {
         tp.y_first) {
       if (!(v >> tp.max_iters)) tp.max_iters = 0;
       if (!(v >> tp.full_side)) tp.full_side = 0;
+      if (!(v >> tp.walk)) tp.walk = 1;
       g_cache[line.substr(0, bar)] = tp;
     }
   }
@@ -71,8 +72,8 @@ int write_cache(const char *path) {
   for (const auto &kv : g_cache)
     f << kv.first << "|" << kv.second.run_bytes << " " << kv.second.vmin_bytes << " "
       << kv.second.smem_bytes << " " << kv.second.rows_min_bytes << " "
-      << kv.second.y_first << " " << kv.second.max_iters << " " << kv.second.full_side
-      << "\n";
+      << kv.second.y_first << " " << kv.second.max_iters << " " << kv.second.full_side << " "
+      << kv.second.walk << "\n";
   return ST_OK;
 }
 
@@ -147,7 +148,20 @@ int autotune(Plan *p, double timeout, TileParams *best) {
   void *user_B = p->args.B;
   p->args.B = scratch;
   std::vector<HpttTile> timed;  // tiles already timed (identical plans skip)
-  for (const TileParams &tp : candidates(elem_bytes(p->args.p.dtype))) {
+  std::vector<TileParams> cands = candidates(elem_bytes(p->args.p.dtype));
+  // After the grid of candidates: the winner again with its two-dim sides
+  // read from tables instead of walked (which is faster depends on the
+  // shape); appended once the winner is known.
+  bool tried_tables = false;
+  for (size_t ci = 0; ci < cands.size() || (found && !tried_tables); ++ci) {
+    if (ci >= cands.size()) {
+      tried_tables = true;  // (a winner without two-dim sides plans the same tile again,
+                            // which the check below skips)
+      TileParams tp = winner;
+      tp.walk = 0;
+      cands.push_back(tp);
+    }
+    const TileParams &tp = cands[ci];
     if (st != ST_OK) break;
     if (timeout > 0) {
       const double el = std::chrono::duration<double>(std::chrono::steady_clock::now() - t_start).count();

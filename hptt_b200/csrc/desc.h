@@ -38,6 +38,18 @@ struct HpttProblem {
   int32_t perm[HPTT_MAX_RANK];
 };
 
+// A thread's slots q = q0 + j * R along a tile side with exactly two dims,
+// walked without the side's offset table: q = d0 + e0 * d1 with offset
+// d0 * s0 + d1 * s1, and a step of R adds r0 = R % e0 to d0 (one carry at
+// most) and step = r0 * s0 + (R / e0) * s1 to the offset; a carry adds
+// carry = s1 - e0 * s0.  e0 == 0: the side is not walked (one dim, three or
+// more, or offsets beyond 32 bits).  mul/shr: fast division by e0.
+struct HpttWalk {
+  int32_t e0, r0, step, carry, s0, s1;
+  uint32_t mul;
+  int32_t shr;
+};
+
 // Tile shape and grid decomposition.
 //
 // A tile is W x X x Y elements:
@@ -112,6 +124,9 @@ struct HpttTile {
   uint32_t tx_mul, ty_mul;
   int32_t tx_shr, ty_shr;
   int32_t pad_;
+  // two-dim sides: the X side's column slots (B offsets, step R2) and the Y
+  // side's row slots (A offsets, step R1)
+  HpttWalk wx, wy;
 };
 
 // One slot of a KIND_TILE offset table (OffT = uint32_t or int64_t).

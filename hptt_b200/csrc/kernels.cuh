@@ -191,6 +191,34 @@ HPTT_HD inline HpttThr thread_consts_1d(const HpttProblem &P, const HpttTile &T,
   return h;
 }
 
+// Walk of a thread's slots along a two-dim tile side (HpttWalk): slot q's
+// first-dim digit and offset, then one step of R.  Unsigned offsets: the
+// last step of a thread may pass the side's end (that slot is not
+// accessed), and wraps instead of overflowing.
+struct WalkPos {
+  int d0;
+  uint32_t off;
+};
+
+HPTT_HD inline WalkPos walk_start(const HpttWalk &w, int q) {
+  const int d1 = fast_div(q, w.mul, w.shr);
+  const int d0 = q - d1 * w.e0;
+  WalkPos p;
+  p.d0 = d0;
+  p.off = static_cast<uint32_t>(d0) * static_cast<uint32_t>(w.s0) +
+          static_cast<uint32_t>(d1) * static_cast<uint32_t>(w.s1);
+  return p;
+}
+
+HPTT_HD inline void walk_step(const HpttWalk &w, WalkPos &p) {
+  p.d0 += w.r0;
+  p.off += static_cast<uint32_t>(w.step);
+  if (p.d0 >= w.e0) {
+    p.d0 -= w.e0;
+    p.off += static_cast<uint32_t>(w.carry);
+  }
+}
+
 // Iterations j >= 0 with q0 + j * R < lim (R > 0): ceil((lim - q0) / R), or 0.
 HPTT_HD inline int valid_iters(int lim, int q0, uint32_t mul, int shr, int R) {
   return lim > q0 ? fast_div(lim - q0 + R - 1, mul, shr) : 0;
@@ -427,26 +455,46 @@ __device__ __forceinline__ void with_trip_count(int n, F &&f) {
   }
 }
 
+// How a tile side yields the offsets of a thread's slots q0 + j * R:
+// q * stride (one dim), a walk (two dims, HpttWalk) or the side's table.
+enum SideKind : int { SIDE_AFFINE = 0, SIDE_WALK = 1, SIDE_TABLE = 2 };
+
+template <int KIND, typename OffT>
+struct SideSlots {
+  int q;        // current slot
+  WalkPos w;    // SIDE_WALK
+  __device__ __forceinline__ SideSlots(int q0, const HpttWalk &wk) : q(q0) {
+    if (KIND == SIDE_WALK) w = walk_start(wk, q0);
+  }
+  // offset of the current slot; `ok`: the slot is inside the side
+  __device__ __forceinline__ OffT offset(bool ok, int stride,
+                                         const HpttTabEnt<OffT> *__restrict__ tab) const {
+    if (KIND == SIDE_AFFINE) return static_cast<OffT>(q * stride);
+    if (KIND == SIDE_WALK) return static_cast<OffT>(w.off);
+    return tab[ok ? q : 0].off;
+  }
+  __device__ __forceinline__ void next(int R, const HpttWalk &wk) {
+    q += R;
+    if (KIND == SIDE_WALK) walk_step(wk, w);
+  }
+};
+
 // Interior tile of a table-driven shape (a side with several dims, or the
 // 64-bit-offset kernel): every chunk coordinate is inside the tensor, so no
-// offset needs a check.  Compile-time trip counts per phase; slots past TY
-// (TX) in an uneven shape are clamped to the last one and repeat it (same
-// element, same value).  A single-dim side takes q * stride instead of its
-// table entry (the tables hold exactly that).  Update tiles read their B
-// values before the barrier, at the same clamped slots as the stores: a
-// repeated slot recomputes the same value from the same original B element,
-// since every B read of the tile precedes every B write.
-template <typename E, int MODE, bool UPD, typename OffT, bool LX, bool LY>
-__device__ __forceinline__ void tile_table_interior(const HpttTile &T, const E *__restrict__ A,
-                                                    E *__restrict__ B,
-                                                    const HpttTabEnt<OffT> *__restrict__ tabY,
-                                                    const HpttTabEnt<OffT> *__restrict__ tabX,
-                                                    const Op<E, MODE, UPD> &op, E *sdata,
-                                                    const HpttThr &th, const TileOrigin &o) {
+// offset needs a check.  Compile-time trip counts per phase (N = J1 or J2);
+// a thread's slot q0 + j*R (q0 < R) can pass the side's end only at its
+// last iteration, which alone is tested.  Every slot is loaded, read and
+// written by exactly one thread.  Update tiles read their B values before
+// the barrier.
+template <typename E, int MODE, bool UPD, typename OffT, int XK, int YK>
+__device__ __forceinline__ void tile_table_interior_k(
+    const HpttTile &T, const E *__restrict__ A, E *__restrict__ B,
+    const HpttTabEnt<OffT> *__restrict__ tabY, const HpttTabEnt<OffT> *__restrict__ tabX,
+    const Op<E, MODE, UPD> &op, E *sdata, const HpttThr &th, const TileOrigin &o) {
   constexpr int J = hptt_jmax_tile(sizeof(E));
   const int LD = T.LD, W = T.W, R1 = T.R1, R2 = T.R2, TX = T.TX, TY = T.TY;
-  const int sY = LY ? static_cast<int>(T.sya) : 0;
-  const int sX = LX ? static_cast<int>(T.sxb) : 0;
+  const int sY = YK == SIDE_AFFINE ? static_cast<int>(T.sya) : 0;
+  const int sX = XK == SIDE_AFFINE ? static_cast<int>(T.sxb) : 0;
   const E *src = A + o.bA + th.inE;
   E *dst = B + o.bB + th.outE2;
   const bool ld = th.active & 1, st = th.active & 2;
@@ -454,14 +502,72 @@ __device__ __forceinline__ void tile_table_interior(const HpttTile &T, const E *
   if (UPD && st) {
     with_trip_count<J>(T.J2, [&](auto n) {
       constexpr int N = decltype(n)::value;
+      SideSlots<XK, OffT> x(th.qs0, T.wx);
 #pragma unroll
       for (int j = 0; j < N; ++j) {
-        const int q = min(th.qs0 + j * R2, TX - 1);
-        bv[UPD ? j : 0] = dst[LX ? static_cast<OffT>(q * sX) : tabX[q].off];
+        const bool ok = j < N - 1 || x.q < TX;
+        const OffT off = x.offset(ok, sX, tabX);
+        if (ok) bv[UPD ? j : 0] = dst[off];
+        x.next(R2, T.wx);
       }
     });
   }
   if (ld) {
+    with_trip_count<J>(T.J1, [&](auto n) {
+      constexpr int N = decltype(n)::value;
+      SideSlots<YK, OffT> y(th.q0, T.wy);
+      E v[N];
+#pragma unroll
+      for (int j = 0; j < N; ++j) {
+        const bool ok = j < N - 1 || y.q < TY;
+        const OffT off = y.offset(ok, sY, tabY);
+        if (ok) v[j] = __ldg(src + off);
+        y.next(R1, T.wy);
+      }
+      E *s = sdata + th.sme + th.q0 * LD;
+#pragma unroll
+      for (int j = 0; j < N; ++j)
+        if (j < N - 1 || th.q0 + j * R1 < TY) s[j * R1 * LD] = v[j];
+    });
+  }
+  __syncthreads();
+  if (st) {
+    with_trip_count<J>(T.J2, [&](auto n) {
+      constexpr int N = decltype(n)::value;
+      SideSlots<XK, OffT> x(th.qs0, T.wx);
+      const E *s = sdata + th.sme2 + th.qs0 * W;
+#pragma unroll
+      for (int j = 0; j < N; ++j) {
+        const bool ok = j < N - 1 || x.q < TX;
+        const OffT off = x.offset(ok, sX, tabX);
+        if (ok) {
+          const E a = s[j * R2 * W];
+          if (UPD)
+            dst[off] = op(a, bv[UPD ? j : 0]);
+          else
+            __stcs(dst + off, op(a, a));
+        }
+        x.next(R2, T.wx);
+      }
+    });
+  }
+}
+
+// The same tile for kernels that keep persistent-loop state (fewer live
+// registers): every phase runs all N iterations with slots past the side's
+// end clamped to the last one, which repeats it (same element, same value);
+// copy and scale tiles only.
+template <typename E, int MODE, bool UPD, typename OffT, bool LX, bool LY>
+__device__ __forceinline__ void tile_table_interior_clamped(
+    const HpttTile &T, const E *__restrict__ A, E *__restrict__ B,
+    const HpttTabEnt<OffT> *__restrict__ tabY, const HpttTabEnt<OffT> *__restrict__ tabX,
+    const Op<E, MODE, UPD> &op, E *sdata, const HpttThr &th, const TileOrigin &o) {
+  constexpr int J = hptt_jmax_tile(sizeof(E));
+  const int LD = T.LD, W = T.W, R1 = T.R1, R2 = T.R2, TX = T.TX, TY = T.TY;
+  const int sY = LY ? static_cast<int>(T.sya) : 0;
+  const int sX = LX ? static_cast<int>(T.sxb) : 0;
+  if (th.active & 1) {
+    const E *src = A + o.bA + th.inE;
     with_trip_count<J>(T.J1, [&](auto n) {
       constexpr int N = decltype(n)::value;
       E v[N];
@@ -476,7 +582,8 @@ __device__ __forceinline__ void tile_table_interior(const HpttTile &T, const E *
     });
   }
   __syncthreads();
-  if (st) {
+  if (th.active & 2) {
+    E *dst = B + o.bB + th.outE2;
     with_trip_count<J>(T.J2, [&](auto n) {
       constexpr int N = decltype(n)::value;
       const E *s = sdata + th.sme2;
@@ -484,13 +591,45 @@ __device__ __forceinline__ void tile_table_interior(const HpttTile &T, const E *
       for (int j = 0; j < N; ++j) {
         const int q = min(th.qs0 + j * R2, TX - 1);
         const E a = s[q * W];
-        E *d = dst + (LX ? static_cast<OffT>(q * sX) : tabX[q].off);
-        if (UPD)
-          *d = op(a, bv[UPD ? j : 0]);
-        else
-          __stcs(d, op(a, a));
+        __stcs(dst + (LX ? static_cast<OffT>(q * sX) : tabX[q].off), op(a, a));
       }
     });
+  }
+}
+
+// Side kinds of a table-driven interior tile, chosen once per tile (uniform);
+// without WALK every multi-dim side reads its table.
+template <typename E, int MODE, bool UPD, typename OffT, bool LX, bool LY, bool WALK>
+__device__ __forceinline__ void tile_table_interior(const HpttTile &T, const E *__restrict__ A,
+                                                    E *__restrict__ B,
+                                                    const HpttTabEnt<OffT> *__restrict__ tabY,
+                                                    const HpttTabEnt<OffT> *__restrict__ tabX,
+                                                    const Op<E, MODE, UPD> &op, E *sdata,
+                                                    const HpttThr &th, const TileOrigin &o) {
+  if constexpr (!WALK) {
+    tile_table_interior_clamped<E, MODE, UPD, OffT, LX, LY>(T, A, B, tabY, tabX, op, sdata, th,
+                                                            o);
+  } else if constexpr (sizeof(OffT) > 4) {
+    tile_table_interior_k<E, MODE, UPD, OffT, SIDE_TABLE, SIDE_TABLE>(T, A, B, tabY, tabX, op,
+                                                                      sdata, th, o);
+  } else if constexpr (!WALK) {
+    tile_table_interior_clamped<E, MODE, UPD, OffT, LX, LY>(T, A, B, tabY, tabX, op, sdata, th,
+                                                            o);
+  } else {
+    constexpr int XA = LX ? SIDE_AFFINE : SIDE_WALK;
+    constexpr int YA = LY ? SIDE_AFFINE : SIDE_WALK;
+    const bool xt = !LX && T.wx.e0 == 0, yt = !LY && T.wy.e0 == 0;
+    if (!xt && !yt)
+      tile_table_interior_k<E, MODE, UPD, OffT, XA, YA>(T, A, B, tabY, tabX, op, sdata, th, o);
+    else if (!xt)
+      tile_table_interior_k<E, MODE, UPD, OffT, XA, SIDE_TABLE>(T, A, B, tabY, tabX, op, sdata,
+                                                                th, o);
+    else if (!yt)
+      tile_table_interior_k<E, MODE, UPD, OffT, SIDE_TABLE, YA>(T, A, B, tabY, tabX, op, sdata,
+                                                                th, o);
+    else
+      tile_table_interior_k<E, MODE, UPD, OffT, SIDE_TABLE, SIDE_TABLE>(T, A, B, tabY, tabX, op,
+                                                                        sdata, th, o);
   }
 }
 
@@ -511,9 +650,10 @@ __device__ __forceinline__ void tile_table_interior(const HpttTile &T, const E *
 // table read (the tables hold exactly these values; the CPU replay checks
 // that).
 // ---------------------------------------------------------------------------
-// UPD_FAST: update tiles may take the bounds-free and clamped forms (more
-// registers: kernels that also keep persistent-loop state turn it off).
-template <typename E, int MODE, bool UPD, typename OffT, bool LX, bool LY, bool UPD_FAST = true>
+// FAST: the forms that need more registers -- update tiles' bounds-free and
+// clamped forms, walked two-dim sides -- are allowed (kernels that also keep
+// persistent-loop state turn it off).
+template <typename E, int MODE, bool UPD, typename OffT, bool LX, bool LY, bool FAST = true>
 __device__ __forceinline__ void tile_one(const HpttProblem &P, const HpttTile &T,
                                          const E *__restrict__ A, E *__restrict__ B,
                                          const unsigned char *__restrict__ tables,
@@ -532,7 +672,7 @@ __device__ __forceinline__ void tile_one(const HpttProblem &P, const HpttTile &T
   const int TX = T.TX, TY = T.TY;
   // Iteration j of a thread covers slot q0 + j*R1 (q0 < R1), so the slot
   // bound q < TY already implies j < J1: the loops test only the slot bound.
-  if (UPD && UPD_FAST && LX && LY && J1 == J && J2 == J) {
+  if (UPD && FAST && LX && LY && J1 == J && J2 == J) {
     // (the clamped edge form needs too many registers with 4-byte
     // elements' 16 iterations; their edge tiles take the general path)
     if (T.even && o.remX >= TX && o.remY >= TY) {
@@ -556,9 +696,12 @@ __device__ __forceinline__ void tile_one(const HpttProblem &P, const HpttTile &T
     tile_clamped<E, MODE, UPD>(T, A, B, op, sdata, th, o);
     return;
   }
-  if ((!UPD || UPD_FAST) && !(LX && LY) && o.remX >= T.xce && o.remY >= T.yce) {
-    tile_table_interior<E, MODE, UPD, OffT, LX, LY>(T, A, B, tabY, tabX, op, sdata, th, o);
-    return;
+  if constexpr (!UPD || FAST) {
+    if (!(LX && LY) && o.remX >= T.xce && o.remY >= T.yce) {
+      tile_table_interior<E, MODE, UPD, OffT, LX, LY, FAST>(T, A, B, tabY, tabX, op, sdata, th,
+                                                            o);
+      return;
+    }
   }
   const bool ld_ok = (th.active & 1) && th.cxe < o.remX;
   const bool st_ok = (th.active & 2) && th.cye2 < o.remY;

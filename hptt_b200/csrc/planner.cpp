@@ -422,6 +422,39 @@ void finish_tables(const HpttProblem &p, HpttTile *t) {
   fast_div_magic(static_cast<uint32_t>(t->R2 > 0 ? t->R2 : 1), &t->r2_mul, &t->r2_shr);
   fast_div_magic(static_cast<uint32_t>(t->TX > 0 ? t->TX : 1), &t->tx_mul, &t->tx_shr);
   fast_div_magic(static_cast<uint32_t>(t->TY > 0 ? t->TY : 1), &t->ty_mul, &t->ty_shr);
+  // two-dim sides of a tile: walk constants (slot order as in tile_maps: Y
+  // dims in input order, X dims in output order)
+  std::memset(&t->wx, 0, sizeof(t->wx));
+  std::memset(&t->wy, 0, sizeof(t->wy));
+  if (t->kind != KIND_TILE || t->big_offsets) return;
+  auto walk = [](HpttWalk *w, int i0, int i1, const int32_t *dims, const int32_t *ext,
+                 const int64_t *stride, int R) {
+    const int64_t e0 = ext[i0], s0 = stride[dims[i0]], s1 = stride[dims[i1]];
+    if (R <= 0 || e0 <= 1) return;
+    const int64_t r0 = R % e0, r1 = R / e0;
+    const int64_t step = r0 * s0 + r1 * s1, carry = s1 - e0 * s0;
+    const int64_t lim = 0x7fffffffLL;
+    if (step > lim || step < -lim || carry > lim || carry < -lim || e0 * s0 > lim ||
+        s1 > lim)
+      return;
+    w->e0 = static_cast<int32_t>(e0);
+    w->r0 = static_cast<int32_t>(r0);
+    w->step = static_cast<int32_t>(step);
+    w->carry = static_cast<int32_t>(carry);
+    w->s0 = static_cast<int32_t>(s0);
+    w->s1 = static_cast<int32_t>(s1);
+    fast_div_magic(static_cast<uint32_t>(e0), &w->mul, &w->shr);
+  };
+  if (t->ny == 2) {
+    const bool in_order = t->yd[0] < t->yd[1];
+    walk(&t->wy, in_order ? 0 : 1, in_order ? 1 : 0, t->yd, t->yt, p.sA, t->R1);
+  }
+  if (t->nx == 2) {
+    int pos[HPTT_MAX_RANK];
+    for (int k = 0; k < p.rank; ++k) pos[p.perm[k]] = k;
+    const bool in_order = pos[t->xd[0]] < pos[t->xd[1]];
+    walk(&t->wx, in_order ? 0 : 1, in_order ? 1 : 0, t->xd, t->xt, p.sB, t->R2);
+  }
 }
 
 int choose_rows(const HpttProblem &p, const TileParams &tp, HpttTile *t) {
@@ -774,6 +807,10 @@ int choose_tile(const HpttProblem &p, const TileParams &tp, int update, HpttTile
   t->thr_off = t->tab2_off + a16(t->TX * ent);
   t->table_bytes = t->thr_off + t->nt * static_cast<int>(sizeof(HpttThr));
   finish_tables(p, t);
+  if (!tp.walk) {
+    std::memset(&t->wx, 0, sizeof(t->wx));
+    std::memset(&t->wy, 0, sizeof(t->wy));
+  }
   return t->num_tiles ? ST_OK : ST_TOO_LARGE;
 }
 
@@ -796,8 +833,10 @@ std::string describe(const HpttProblem &p, const HpttTile &t) {
   for (int i = 0; i < t.nx; ++i) os << (i ? "," : "") << t.xd[i] << ":" << t.xt[i];
   os << "} Y{";
   for (int i = 0; i < t.ny; ++i) os << (i ? "," : "") << t.yd[i] << ":" << t.yt[i];
-  os << "} TX=" << t.TX << " TY=" << t.TY << " LD=" << t.LD << "\n  tiles: " << t.num_tiles
-     << ", smem/CTA: " << t.smem_bytes << " B\n";
+  os << "} TX=" << t.TX << " TY=" << t.TY << " LD=" << t.LD;
+  if (t.wx.e0 || t.wy.e0)
+    os << " walked:" << (t.wx.e0 ? " X" : "") << (t.wy.e0 ? " Y" : "");
+  os << "\n  tiles: " << t.num_tiles << ", smem/CTA: " << t.smem_bytes << " B\n";
   return os.str();
 }
 

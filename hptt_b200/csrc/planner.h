@@ -48,6 +48,8 @@ struct TileParams {
                            // 2 = the whole Y extent, shrinking the other side
                            // (short rows that are not sector-aligned then
                            // become one contiguous range per tile)
+  int walk = 1;            // two-dim tile sides: walk the slot offsets (1) or
+                           // read the side's table (0); HpttWalk
 };
 
 // Reference argument guard (src/hptt.cc:25-56) plus the one check the

@@ -54,10 +54,13 @@ bool b_is_inner(const Layout &L, int64_t ib) {
   return true;
 }
 
+// fast: replay the single-transpose kernel (tile_one with FAST); else the
+// persistent batch kernels (FAST off: no update fast forms, clamped
+// table-driven interiors, no walked sides).
 template <typename OffT>
 int replay_tile(const HpttProblem &P, const HpttTile &T, int update, const Layout &L,
                 const std::vector<unsigned char> &tab, std::vector<uint8_t> &writes,
-                uint64_t *checked) {
+                uint64_t *checked, bool fast) {
   const int esz = elem_bytes(P.dtype);
   const int J = hptt_jmax_tile(esz);
   (void)update;
@@ -114,13 +117,36 @@ int replay_tile(const HpttProblem &P, const HpttTile &T, int update, const Layou
   // row/column (kernels.cuh: tile_clamped, tile_full_upd), so an iteration
   // past the edge repeats a slot with the same element
   const bool clamped_kind =
-      lx && ly && (!update || (T.J1 == J && T.J2 == J && elem_bytes(P.dtype) > 4));
-  // tiles with a multi-dim side (copy, scale and update): interior tiles run
-  // compile-time loops over the tables (kernels.cuh: tile_table_interior),
-  // slots past TY (TX) clamped to the last one; update tiles read B at the
-  // store slots before the barrier
-  const bool table_kind = !(lx && ly);
-  const bool tracks = clamped_kind || table_kind;
+      lx && ly && (!update || (fast && T.J1 == J && T.J2 == J && elem_bytes(P.dtype) > 4));
+  // tiles with a multi-dim side, interior tiles.  Single-transpose kernel
+  // (kernels.cuh: tile_table_interior_k): copy, scale and update tiles run
+  // exact trip counts, a thread's last slot alone tested against the side's
+  // end, offsets from the tables, from q * stride (one dim) or from a walk
+  // (two dims, HpttWalk -- replayed here against the tables).  Batch kernels
+  // (tile_table_interior_clamped): copy/scale tiles only, every slot past
+  // the end clamped to the last one.
+  const bool table_kind = fast && !(lx && ly);
+  const bool table_clamped_kind = !fast && !update && !(lx && ly);
+  const bool tracks = clamped_kind || table_clamped_kind;
+  // walked sides: the walk must give the table's offset at every slot a
+  // thread reaches (kernels.cuh: walk_start / walk_step)
+  if (fast && !T.big_offsets) {
+    for (int side = 0; side < 2; ++side) {
+      const HpttWalk &w = side ? T.wx : T.wy;
+      if (w.e0 == 0) continue;
+      if ((side ? T.nx : T.ny) != 2) return 154;
+      const int R = side ? T.R2 : T.R1, N = side ? T.J2 : T.J1, lim = side ? T.TX : T.TY;
+      const Ent *tb = side ? tabX : tabY;
+      for (int q0 = 0; q0 < R; ++q0) {
+        WalkPos wp = walk_start(w, q0);
+        for (int j = 0; j < N; ++j) {
+          const int q = q0 + j * R;
+          if (q < lim && wp.off != static_cast<uint32_t>(tb[q].off)) return 155;
+          walk_step(w, wp);
+        }
+      }
+    }
+  }
   std::vector<int64_t> writer(tracks ? static_cast<size_t>(L.nB) : 0, -1);
   std::vector<uint32_t> writer_tile(tracks ? static_cast<size_t>(L.nB) : 0, 0);
   for (uint32_t tile = 0; tile < T.num_tiles; ++tile) {
@@ -129,7 +155,52 @@ int replay_tile(const HpttProblem &P, const HpttTile &T, int update, const Layou
     const int limQY = (ly && T.yc >= 0 && o.remY < T.TY) ? o.remY : T.TY;
     const int limQX = (lx && T.xc >= 0 && o.remX < T.TX) ? o.remX : T.TX;
     const bool interior = T.even && o.remX >= T.TX && o.remY >= T.TY;
-    const bool table_interior = table_kind && o.remX >= T.xce && o.remY >= T.yce;
+    const bool inside = o.remX >= T.xce && o.remY >= T.yce;
+    if (table_kind && inside) {
+      // predicated exact-trip-count form: every slot once
+      for (int t = 0; t < T.nt; ++t) {
+        const HpttThr &th = thr[t];
+        if (!(th.active & 1)) continue;
+        for (int j = 0; j < T.J1; ++j) {
+          const int q = th.q0 + j * T.R1;
+          if (q >= T.TY) {
+            if (j != T.J1 - 1) return 156;  // only the last iteration may pass the end
+            continue;
+          }
+          if (!(tabY[q].c < o.remY) || th.cxe >= o.remX) return 157;
+          const int64_t si = static_cast<int64_t>(q) * T.LD + th.sme;
+          if (si < 0 || si >= smem_elems) return 158;
+          if (slot[si] >= 0) return 159;  // two writers of one slot
+          const int64_t ia = o.bA + th.inE + static_cast<int64_t>(tabY[q].off);
+          if (ia < 0 || ia >= L.nA) return 160;
+          slot[si] = ia;
+        }
+      }
+      for (int t = 0; t < T.nt; ++t) {
+        const HpttThr &th = thr[t];
+        if (!(th.active & 2)) continue;
+        for (int j = 0; j < T.J2; ++j) {
+          const int q = th.qs0 + j * T.R2;
+          if (q >= T.TX) {
+            if (j != T.J2 - 1) return 161;
+            continue;
+          }
+          if (!(tabX[q].c < o.remX) || th.cye2 >= o.remY) return 162;
+          const int64_t si = static_cast<int64_t>(th.sme2) + static_cast<int64_t>(q) * T.W;
+          if (si < 0 || si >= smem_elems) return 163;
+          const int64_t ia = slot[si];
+          if (ia < 0) return 164;  // reads a slot no load wrote
+          const int64_t ib = o.bB + th.outE2 + static_cast<int64_t>(tabX[q].off);
+          if (ib < 0 || ib >= L.nB) return 165;
+          if (map_a_to_b(L, ia) != ib) return 166;
+          if (writes[ib] != 0) return 167;  // one write per element (B read once too)
+          writes[ib] = 1;
+          ++*checked;
+        }
+      }
+      continue;
+    }
+    const bool table_interior = table_clamped_kind && inside;
     if ((clamped_kind && !interior) || table_interior) {
       const int limR = table_interior ? T.TY : (T.yc >= 0 && o.remY < T.TY) ? o.remY : T.TY;
       const int limC = table_interior ? T.TX : (T.xc >= 0 && o.remX < T.TX) ? o.remX : T.TX;
@@ -327,19 +398,23 @@ extern "C" int hptt_cuda_debug_check_indexing(int dtype, uint32_t rank, const ui
     if (st != ST_OK) return st;
     std::vector<unsigned char> tab;
     build_tables(P, T, &tab);
-    std::vector<uint8_t> writes(static_cast<size_t>(L.nB), 0);
-    uint64_t n = 0;
-    int rc;
-    if (T.kind == KIND_TILE)
-      rc = T.big_offsets ? replay_tile<int64_t>(P, T, update, L, tab, writes, &n)
-                         : replay_tile<uint32_t>(P, T, update, L, tab, writes, &n);
-    else
-      rc = T.big_offsets ? replay_rows<int64_t>(P, T, L, tab, writes, &n)
-                         : replay_rows<uint32_t>(P, T, L, tab, writes, &n);
-    if (rc != 0) return 1000 + rc;
-    for (int64_t ib = 0; ib < L.nB; ++ib)
-      if (static_cast<bool>(writes[ib]) != b_is_inner(L, ib)) return 1300;
-    if (checked) *checked = n;
+    // the single-transpose kernel, then (tiles) the batch kernels' forms
+    for (int model = 0; model < (T.kind == KIND_TILE ? 2 : 1); ++model) {
+      std::vector<uint8_t> writes(static_cast<size_t>(L.nB), 0);
+      uint64_t n = 0;
+      int rc;
+      const bool fast = model == 0;
+      if (T.kind == KIND_TILE)
+        rc = T.big_offsets ? replay_tile<int64_t>(P, T, update, L, tab, writes, &n, fast)
+                           : replay_tile<uint32_t>(P, T, update, L, tab, writes, &n, fast);
+      else
+        rc = T.big_offsets ? replay_rows<int64_t>(P, T, L, tab, writes, &n)
+                           : replay_rows<uint32_t>(P, T, L, tab, writes, &n);
+      if (rc != 0) return 1000 + rc + (model ? 500 : 0);
+      for (int64_t ib = 0; ib < L.nB; ++ib)
+        if (static_cast<bool>(writes[ib]) != b_is_inner(L, ib)) return 1300;
+      if (checked) *checked = n;
+    }
   }
   return 0;
 }
