@@ -38,8 +38,8 @@ std::string gpu_name() {
 const char *env_path() { return std::getenv("HPTT_B200_TUNE_CACHE"); }
 
 // Cache file: one line per key,
-// "key|run vmin smem rows_min y_first iters full_side walk"
-// (missing trailing fields read as 0, walk as 1).
+// "key|run vmin smem rows_min y_first iters full_side walk upd_exact"
+// (missing trailing fields read as 0, walk and upd_exact as 1).
 void read_cache_stream(std::istream &f) {
   std::string line;
   while (std::getline(f, line)) {
@@ -52,6 +52,7 @@ void read_cache_stream(std::istream &f) {
       if (!(v >> tp.max_iters)) tp.max_iters = 0;
       if (!(v >> tp.full_side)) tp.full_side = 0;
       if (!(v >> tp.walk)) tp.walk = 1;
+      if (!(v >> tp.upd_exact)) tp.upd_exact = 1;
       g_cache[line.substr(0, bar)] = tp;
     }
   }
@@ -73,7 +74,7 @@ int write_cache(const char *path) {
     f << kv.first << "|" << kv.second.run_bytes << " " << kv.second.vmin_bytes << " "
       << kv.second.smem_bytes << " " << kv.second.rows_min_bytes << " "
       << kv.second.y_first << " " << kv.second.max_iters << " " << kv.second.full_side << " "
-      << kv.second.walk << "\n";
+      << kv.second.walk << " " << kv.second.upd_exact << "\n";
   return ST_OK;
 }
 
@@ -149,16 +150,20 @@ int autotune(Plan *p, double timeout, TileParams *best) {
   p->args.B = scratch;
   std::vector<HpttTile> timed;  // tiles already timed (identical plans skip)
   std::vector<TileParams> cands = candidates(elem_bytes(p->args.p.dtype));
-  // After the grid of candidates: the winner again with its two-dim sides
-  // read from tables instead of walked (which is faster depends on the
-  // shape); appended once the winner is known.
-  bool tried_tables = false;
-  for (size_t ci = 0; ci < cands.size() || (found && !tried_tables); ++ci) {
+  // After the grid of candidates, two alternative forms of the winner, each
+  // kept only if faster (which wins depends on the shape): its two-dim
+  // sides read from tables instead of walked, then, for update tiles, the
+  // general predicated path instead of exact trip counts.  A winner without
+  // such sides or tiles plans the same tile again, which the check below
+  // skips.
+  int alt = 0;
+  for (size_t ci = 0; ci < cands.size() || (found && alt < 2); ++ci) {
     if (ci >= cands.size()) {
-      tried_tables = true;  // (a winner without two-dim sides plans the same tile again,
-                            // which the check below skips)
       TileParams tp = winner;
-      tp.walk = 0;
+      if (alt++ == 0)
+        tp.walk = 0;
+      else
+        tp.upd_exact = 0;
       cands.push_back(tp);
     }
     const TileParams &tp = cands[ci];

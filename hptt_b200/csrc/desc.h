@@ -123,7 +123,9 @@ struct HpttTile {
   // with W == 1 are computed from threadIdx instead of read from the table
   uint32_t tx_mul, ty_mul;
   int32_t tx_shr, ty_shr;
-  int32_t pad_;
+  // update tiles with single-dim sides: 1 = interior tiles run exact trip
+  // counts (tile_table_interior_k), 0 = the general predicated path
+  int32_t upd_exact;
   // two-dim sides: the X side's column slots (B offsets, step R2) and the Y
   // side's row slots (A offsets, step R1)
   HpttWalk wx, wy;

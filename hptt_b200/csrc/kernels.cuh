@@ -697,7 +697,9 @@ __device__ __forceinline__ void tile_one(const HpttProblem &P, const HpttTile &T
     return;
   }
   if constexpr (!UPD || FAST) {
-    if (!(LX && LY) && o.remX >= T.xce && o.remY >= T.yce) {
+    // interior tiles with a multi-dim side, and update tiles with single-dim
+    // sides that the forms above did not take
+    if ((!(LX && LY) || (UPD && T.upd_exact)) && o.remX >= T.xce && o.remY >= T.yce) {
       tile_table_interior<E, MODE, UPD, OffT, LX, LY, FAST>(T, A, B, tabY, tabX, op, sdata, th,
                                                             o);
       return;
@@ -792,6 +794,41 @@ __device__ __forceinline__ void rows_one(const HpttProblem &P, const HpttTile &T
   const E *src = A + o.bA + col * P.sA[0];
   E *dst = B + o.bB + col * P.sB[0];
   const int R1 = T.R1;
+  if (rows_limit_y(T, o) == T.TY) {
+    // Interior tile: compile-time trip count J1; a thread's row y0 + j*R1
+    // (y0 < R1) can pass TY only at its last iteration.  One Y dim: row
+    // offsets y * stride instead of the tables (which hold exactly that).
+    const int y0 = s.y0, TY = T.TY;
+    const bool one = T.ny == 1;
+    const int64_t sa = T.sya, sb = T.syb;
+    with_trip_count<J>(T.J1, [&](auto nn) {
+      constexpr int N = decltype(nn)::value;
+      Vec<E, VEC> av[N];
+      Vec<E, VEC> bv[UPD ? N : 1];
+#pragma unroll
+      for (int j = 0; j < N; ++j) {
+        const int y = y0 + j * R1;
+        if (j < N - 1 || y < TY) {
+          av[j] = ld_vec<E, VEC>(src + (one ? y * sa : static_cast<int64_t>(__ldg(tabA + y))));
+          if (UPD)
+            bv[UPD ? j : 0] =
+                ld_vec_rw<E, VEC>(dst + (one ? y * sb : static_cast<int64_t>(__ldg(tabB + y))));
+        }
+      }
+#pragma unroll
+      for (int j = 0; j < N; ++j) {
+        const int y = y0 + j * R1;
+        if (j < N - 1 || y < TY) {
+          Vec<E, VEC> r;
+#pragma unroll
+          for (int k = 0; k < VEC; ++k)
+            r.v[k] = op(av[j].v[k], UPD ? bv[UPD ? j : 0].v[k] : av[j].v[k]);
+          st_vec<E, VEC>(dst + (one ? y * sb : static_cast<int64_t>(__ldg(tabB + y))), r);
+        }
+      }
+    });
+    return;
+  }
   Vec<E, VEC> av[J];
   Vec<E, VEC> bv[J];
 #pragma unroll

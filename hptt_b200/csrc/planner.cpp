@@ -811,6 +811,7 @@ int choose_tile(const HpttProblem &p, const TileParams &tp, int update, HpttTile
     std::memset(&t->wx, 0, sizeof(t->wx));
     std::memset(&t->wy, 0, sizeof(t->wy));
   }
+  t->upd_exact = tp.upd_exact ? 1 : 0;
   return t->num_tiles ? ST_OK : ST_TOO_LARGE;
 }
 

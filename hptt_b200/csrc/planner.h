@@ -50,6 +50,9 @@ struct TileParams {
                            // become one contiguous range per tile)
   int walk = 1;            // two-dim tile sides: walk the slot offsets (1) or
                            // read the side's table (0); HpttWalk
+  int upd_exact = 1;       // update tiles with single-dim sides: exact trip
+                           // counts in interior tiles (1) or the general
+                           // predicated path (0); HpttTile::upd_exact
 };
 
 // Reference argument guard (src/hptt.cc:25-56) plus the one check the

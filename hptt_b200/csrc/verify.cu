@@ -125,7 +125,7 @@ int replay_tile(const HpttProblem &P, const HpttTile &T, int update, const Layou
   // (two dims, HpttWalk -- replayed here against the tables).  Batch kernels
   // (tile_table_interior_clamped): copy/scale tiles only, every slot past
   // the end clamped to the last one.
-  const bool table_kind = fast && !(lx && ly);
+  const bool table_kind = fast && (!(lx && ly) || (update && T.upd_exact));
   const bool table_clamped_kind = !fast && !update && !(lx && ly);
   const bool tracks = clamped_kind || table_clamped_kind;
   // walked sides: the walk must give the table's offset at every slot a
@@ -156,7 +156,11 @@ int replay_tile(const HpttProblem &P, const HpttTile &T, int update, const Layou
     const int limQX = (lx && T.xc >= 0 && o.remX < T.TX) ? o.remX : T.TX;
     const bool interior = T.even && o.remX >= T.TX && o.remY >= T.TY;
     const bool inside = o.remX >= T.xce && o.remY >= T.yce;
-    if (table_kind && inside) {
+    // update tiles with single-dim sides that tile_interior_upd or
+    // tile_full_upd take first (kernels.cuh: tile_one)
+    const bool upd_fast_form = update && fast && lx && ly && T.J1 == J && T.J2 == J &&
+                               ((T.even && interior) || esz > 4);
+    if (table_kind && inside && !upd_fast_form) {
       // predicated exact-trip-count form: every slot once
       for (int t = 0; t < T.nt; ++t) {
         const HpttThr &th = thr[t];
@@ -320,6 +324,12 @@ int replay_rows(const HpttProblem &P, const HpttTile &T, const Layout &L,
   if (vec > 1 && (P.sA[0] != 1 || P.sB[0] != 1)) return 204;
   const OffT *tabA = reinterpret_cast<const OffT *>(tab.data());
   const OffT *tabB = reinterpret_cast<const OffT *>(tab.data() + T.tab2_off);
+  // one Y dim: interior tiles take y * stride instead of the tables
+  if (T.ny == 1) {
+    for (int y = 0; y < T.TY; ++y)
+      if (static_cast<int64_t>(tabA[y]) != y * T.sya || static_cast<int64_t>(tabB[y]) != y * T.syb)
+        return 214;
+  }
   for (uint32_t tile = 0; tile < T.num_tiles; ++tile) {
     const TileOrigin o = tile_origin(P, T, tile);
     const int limY = rows_limit_y(T, o);
@@ -329,6 +339,8 @@ int replay_rows(const HpttProblem &P, const HpttTile &T, const Layout &L,
       const int64_t col = static_cast<int64_t>(s.e) * vec;
       if (col >= o.remX) continue;
       const int n = std::min(T.J1, valid_iters(limY, s.y0, T.r1_mul, T.r1_shr, T.R1));
+      // interior tiles run J1 iterations and test only the last one
+      if (limY == T.TY && n < T.J1 - 1) return 213;
       for (int j = 0; j < J; ++j) {
         const int y = s.y0 + j * T.R1;
         if (!(j < n)) continue;
@@ -387,12 +399,16 @@ extern "C" int hptt_cuda_debug_check_indexing(int dtype, uint32_t rank, const ui
   }
   L.nB = s;
   // every planner knob the tuner tries: side order, both update settings,
-  // both per-thread iteration limits, the whole-extent options
+  // both per-thread iteration limits, the whole-extent options, tables or
+  // walks for two-dim sides, exact or predicated update interiors
   for (int variant = 0; variant < 24; ++variant) {
     const int update = variant & 1;
     tp.y_first = (variant >> 1) & 1;
     tp.max_iters = ((variant >> 2) & 1) ? hptt_jmax_tile(elem_bytes(P.dtype)) / 2 : 0;
     tp.full_side = variant >> 3;
+    // the tuner's alternative forms, each in half of the variants
+    tp.walk = ((variant >> 2) & 1) ? 0 : 1;
+    tp.upd_exact = ((variant >> 1) & 1) ? 0 : 1;
     HpttTile T;
     st = choose_tile(P, tp, update, &T);
     if (st != ST_OK) return st;

@@ -192,6 +192,52 @@ def test_tuned_plan_matches():
     assert_same(got, oracle_run("f64", size, perm, 2.3, 4.2, a, b0), "f64", "tuned")
 
 
+# Shapes whose tiles have two-dim sides (walked or read from tables) or
+# single-dim sides with an update (exact trip counts or the predicated path).
+FORM_SHAPES = [
+    ("f32", [30, 4, 34, 6, 5, 3], [2, 5, 1, 4, 0, 3]),
+    ("f32", [54, 19, 6, 5, 4, 7], [3, 1, 5, 2, 4, 0]),
+    ("f64", [17, 50, 46, 3, 2, 4], [4, 2, 3, 5, 1, 0]),
+    ("f32", [65, 448, 17], [1, 0, 2]),
+    ("f32", [49, 88, 93, 6], [1, 3, 0, 2]),
+    ("c64", [12, 4, 4, 11, 19, 13], [4, 0, 5, 3, 1, 2]),
+    ("c128", [6, 6, 15, 77, 6, 3], [1, 2, 5, 0, 3, 4]),
+]
+
+
+@pytest.mark.parametrize("name,size,perm", FORM_SHAPES)
+@pytest.mark.parametrize("al,be", [(1.0, 0.0), (2.3, 4.2)])
+def test_tile_forms_match(tmp_path, name, size, perm, al, be):
+    """The tuner's alternative tile forms, each forced through the tune cache
+    (tune once, rewrite the entry's walk / upd_exact fields, reload): every
+    form bit-exact against the oracle."""
+    rng = np.random.default_rng(17)
+    n_in, n_out = footprint(size, perm)
+    a = seeded(rng, n_in, name)
+    b0 = seeded(rng, n_out, name)
+    want = oracle_run(name, size, perm, al, be, a, b0)
+    h.tune_cache_clear()
+    try:
+        got = gpu_run(name, size, perm, al, be, a, b0, tuning_timeout=-1.0)
+        assert_same(got, want, name, f"tuned {size} {perm}")
+        path = tmp_path / "forms.cache"
+        h.tune_cache_save(str(path))
+        (line,) = path.read_text().splitlines()
+        key, fields = line.split("|")
+        f = fields.split()
+        assert len(f) == 9
+        for walk in (0, 1):
+            for exact in (0, 1):
+                f[7], f[8] = str(walk), str(exact)
+                path.write_text(key + "|" + " ".join(f) + "\n")
+                h.tune_cache_clear()
+                h.tune_cache_load(str(path))
+                got = gpu_run(name, size, perm, al, be, a, b0)
+                assert_same(got, want, name, f"{size} {perm} walk={walk} exact={exact}")
+    finally:
+        h.tune_cache_clear()
+
+
 # --------------------------------------------------------------------------
 # Workloads at full size
 # --------------------------------------------------------------------------
