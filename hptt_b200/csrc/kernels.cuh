@@ -796,11 +796,10 @@ __device__ __forceinline__ void rows_one(const HpttProblem &P, const HpttTile &T
   const int R1 = T.R1;
   if (rows_limit_y(T, o) == T.TY) {
     // Interior tile: compile-time trip count J1; a thread's row y0 + j*R1
-    // (y0 < R1) can pass TY only at its last iteration.  One Y dim: row
-    // offsets y * stride instead of the tables (which hold exactly that).
+    // (y0 < R1) can pass TY only at its last iteration.  Row offsets come
+    // from the tables even for one Y dim: a warp's lanes read the same entry
+    // (one broadcast), which measured faster than 64-bit y * stride.
     const int y0 = s.y0, TY = T.TY;
-    const bool one = T.ny == 1;
-    const int64_t sa = T.sya, sb = T.syb;
     with_trip_count<J>(T.J1, [&](auto nn) {
       constexpr int N = decltype(nn)::value;
       Vec<E, VEC> av[N];
@@ -809,10 +808,8 @@ __device__ __forceinline__ void rows_one(const HpttProblem &P, const HpttTile &T
       for (int j = 0; j < N; ++j) {
         const int y = y0 + j * R1;
         if (j < N - 1 || y < TY) {
-          av[j] = ld_vec<E, VEC>(src + (one ? y * sa : static_cast<int64_t>(__ldg(tabA + y))));
-          if (UPD)
-            bv[UPD ? j : 0] =
-                ld_vec_rw<E, VEC>(dst + (one ? y * sb : static_cast<int64_t>(__ldg(tabB + y))));
+          av[j] = ld_vec<E, VEC>(src + __ldg(tabA + y));
+          if (UPD) bv[UPD ? j : 0] = ld_vec_rw<E, VEC>(dst + __ldg(tabB + y));
         }
       }
 #pragma unroll
@@ -823,7 +820,7 @@ __device__ __forceinline__ void rows_one(const HpttProblem &P, const HpttTile &T
 #pragma unroll
           for (int k = 0; k < VEC; ++k)
             r.v[k] = op(av[j].v[k], UPD ? bv[UPD ? j : 0].v[k] : av[j].v[k]);
-          st_vec<E, VEC>(dst + (one ? y * sb : static_cast<int64_t>(__ldg(tabB + y))), r);
+          st_vec<E, VEC>(dst + __ldg(tabB + y), r);
         }
       }
     });

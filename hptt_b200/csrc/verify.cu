@@ -324,12 +324,6 @@ int replay_rows(const HpttProblem &P, const HpttTile &T, const Layout &L,
   if (vec > 1 && (P.sA[0] != 1 || P.sB[0] != 1)) return 204;
   const OffT *tabA = reinterpret_cast<const OffT *>(tab.data());
   const OffT *tabB = reinterpret_cast<const OffT *>(tab.data() + T.tab2_off);
-  // one Y dim: interior tiles take y * stride instead of the tables
-  if (T.ny == 1) {
-    for (int y = 0; y < T.TY; ++y)
-      if (static_cast<int64_t>(tabA[y]) != y * T.sya || static_cast<int64_t>(tabB[y]) != y * T.syb)
-        return 214;
-  }
   for (uint32_t tile = 0; tile < T.num_tiles; ++tile) {
     const TileOrigin o = tile_origin(P, T, tile);
     const int limY = rows_limit_y(T, o);
