@@ -14,10 +14,13 @@ constexpr int kNT = 256;
 
 // One CTA per tile.  The arguments live in the parameter space
 // (__grid_constant__) and are read through a const reference.  Register
-// budgets: 6 resident CTAs per SM for the copy/scale tiles (the shared-memory
-// limit at 32 KB a tile), 4 when B is read too.
+// budgets: 8 resident CTAs per SM for 4-byte copy/scale tiles (32 registers;
+// measured +0.3 % over the sweep, up to +8 % on short-run shapes), 6 for
+// wider elements (the shared-memory limit at 32 KB a tile; at 32 registers
+// they spill), 4 when B is read too.
 template <typename E, int MODE, bool UPD, typename OffT, bool LX, bool LY>
-__global__ void __launch_bounds__(kNT, UPD ? 4 : 6) k_tile(const __grid_constant__ HpttArgs args) {
+__global__ void __launch_bounds__(kNT, UPD ? 4 : (sizeof(E) <= 4 ? 8 : 6))
+    k_tile(const __grid_constant__ HpttArgs args) {
   extern __shared__ __align__(16) unsigned char smem[];
   const Scal sc{args.alpha[0], args.alpha[1], args.beta[0], args.beta[1]};
   const Op<E, MODE, UPD> op(sc);
