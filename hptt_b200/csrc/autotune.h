@@ -1,4 +1,5 @@
-// Tile-shape autotuner with a per-(dtype, rank, perm, size class) cache.
+// Tile-shape autotuner with a per-(dtype, rank, perm, size class, extent
+// classes) cache.
 //
 // Replaces the reference's timing tuner PlanTrans::tuning_
 // (inc/hptt/plan/plan_trans.tcc:33-67).  The reference times its candidates
@@ -22,7 +23,8 @@ int autotune(Plan *p, double timeout, TileParams *best);
 // Cached parameters for this plan's key, if any.
 bool autotune_cache_lookup(const Plan *p, TileParams *out);
 
-// Cache key text (dtype, fused rank, fused perm, size class).
+// Cache key text (GPU, dtype, fused rank, fused perm, size class, B read,
+// extent class of every fused dim).
 std::string autotune_key(const Plan *p);
 
 // Load/save the cache file named by HPTT_B200_TUNE_CACHE (no-op if unset)

@@ -6,7 +6,8 @@ anything (plans created with tuning_timeout == 0 look the cache up).
         [--workloads sweep,plain,hard,batch] [--batch-count 4096]
 
 Entries are keyed by (GPU name, dtype, fused rank, fused perm, size class,
-whether B is read), so one entry serves every shape of that class.  Buffers
+whether B is read, floor(log2) of every fused extent), so one entry serves
+every shape of that class.  Buffers
 are allocated per case and freed before the next one.
 """
 from __future__ import annotations

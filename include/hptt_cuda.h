@@ -371,7 +371,8 @@ int hptt_cuda_contract_describe(hptt_cuda_contract_t plan, char *buf, size_t len
 int hptt_cuda_contract_destroy(hptt_cuda_contract_t plan);
 
 /* Autotune cache: the tile parameters the tuner picked, one entry per
- * (GPU name, dtype, fused rank, fused perm, size class, B read).  Plans
+ * (GPU name, dtype, fused rank, fused perm, size class, B read, extent
+ * class floor(log2) of every fused dim).  Plans
  * created with tuning_timeout == 0 use a matching entry instead of the
  * heuristic.  The file named by the environment variable
  * HPTT_B200_TUNE_CACHE is read on first use and rewritten after every tuning
