@@ -333,6 +333,10 @@ int hptt_cuda_server_destroy(hptt_cuda_server_t server);
  *                   bytes hptt_cuda_contract_inspect reports
  *                   (HPTT_ERR_BUDGET otherwise); NULL: the plan allocates
  *                   and frees its own.
+ * Like a transpose plan, one contraction plan is not executed from two host
+ * threads at once; execs on different streams must not overlap (they share
+ * the workspace).  destroy may be called with work in flight: it waits for
+ * the device before freeing memory.
  */
 typedef struct hptt_cuda_contract_s *hptt_cuda_contract_t;
 typedef struct {
