@@ -38,10 +38,13 @@ void set_scalars(HpttArgs *a, const double *alpha, const double *beta,
     upd = std::fabs(a->beta[0]) >= 1e-16;
   }
   a->update = upd ? 1 : 0;
-  const bool alpha_one = use_cplx ? (a->alpha[0] == 1.0 && a->alpha[1] == 0.0)
-                                  : ((a->p.dtype == DT_F32 || a->p.dtype == DT_C64)
-                                         ? static_cast<float>(a->alpha[0]) == 1.0f
-                                         : a->alpha[0] == 1.0);
+  // A bit copy equals fl(1 * a) per component for real scalars only.  With
+  // complex scalars alpha = 1+0i still computes fl(fl(1*xr) - fl(0*xi)) and
+  // fl(fl(1*xi) + fl(0*xr)): -0 parts can turn +0, and an infinite or NaN
+  // part makes the other part NaN, so that mode never takes the copy.
+  const bool alpha_one = !use_cplx && ((a->p.dtype == DT_F32 || a->p.dtype == DT_C64)
+                                           ? static_cast<float>(a->alpha[0]) == 1.0f
+                                           : a->alpha[0] == 1.0);
   if (!upd && alpha_one)
     a->mode = MODE_COPY;
   else

@@ -2,25 +2,29 @@
 //
 // hptt_cuda_plan_create keeps each plan's offset tables (a few KB) in a
 // device buffer it obtains with cudaMalloc.  Some callers cannot allocate
-// device memory at the moment they need a transpose: code that records work
-// while a stream is being captured, runtimes whose device memory is handed
-// out only by their own pool or arena, and jobs held to a fixed memory
-// budget.  hptt_cuda_transpose_noalloc serves them: it plans on the host,
-// copies the tables into a fixed array compiled into this library, and
-// launches the same kernel -- without cudaMalloc, cudaFree or any other
-// device allocator.
+// device memory at the moment they need a transpose: runtimes whose device
+// memory is handed out only by their own pool or arena (a cudaMalloc behind
+// the pool's back would break its accounting or fail under its reservation),
+// and jobs held to a fixed device-memory budget.  hptt_cuda_transpose_noalloc
+// serves them: it plans on the host, copies the tables into a fixed array
+// compiled into this library, and launches the same kernel -- without
+// cudaMalloc, cudaFree or any other device allocator.
 //
 // The array is a file-scope __device__ variable of HPTT_NOALLOC_TABLE_BYTES
 // bytes; every GPU that loads the library holds it until the process exits.
 // In host code its name only stands in for it, so its device address is
 // looked up once per device, with that device current, by
-// cudaGetSymbolAddress, and that address is what the kernel receives.
+// cudaGetSymbolAddress, and that address is what the kernel receives.  The
+// address is kept for the life of the process: after cudaDeviceReset (which
+// destroys the context that holds the array) this entry point must not be
+// called again in that process.
 #include <cuda_runtime.h>
 
 #include <mutex>
 #include <vector>
 
 #include "../../include/hptt_cuda.h"
+#include "autotune.h"
 #include "launch.h"
 #include "plan.h"
 #include "planner.h"
@@ -79,7 +83,22 @@ extern "C" int hptt_cuda_transpose_noalloc(int dtype, uint32_t rank, const uint3
   a.B = out;
   set_scalars(&a, alpha, beta, complex_scalars);
 
+  // The tile the plan path would run: the autotune cache's entry for this
+  // problem when there is one (its key needs only the fused problem, the
+  // element count and whether B is read), else the planner's default.  An
+  // entry whose tables would not fit the array falls back to the default.
   TileParams tp;
+  {
+    Plan probe;
+    probe.args = a;
+    probe.elements = 1;
+    for (uint32_t d = 0; d < rank; ++d) probe.elements *= in_size[d];
+    TileParams cached;
+    if (autotune_cache_lookup(&probe, &cached) &&
+        choose_tile(a.p, cached, a.update, &a.t) == ST_OK &&
+        a.t.table_bytes <= HPTT_NOALLOC_TABLE_BYTES)
+      tp = cached;
+  }
   st = choose_tile(a.p, tp, a.update, &a.t);
   if (st != ST_OK) return st;
   int vec = a.t.kind == KIND_ROWS ? a.t.vec : 1;

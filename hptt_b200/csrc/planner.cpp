@@ -837,7 +837,8 @@ std::string describe(const HpttProblem &p, const HpttTile &t) {
   os << "} TX=" << t.TX << " TY=" << t.TY << " LD=" << t.LD;
   if (t.wx.e0 || t.wy.e0)
     os << " walked:" << (t.wx.e0 ? " X" : "") << (t.wy.e0 ? " Y" : "");
-  os << "\n  tiles: " << t.num_tiles << ", smem/CTA: " << t.smem_bytes << " B\n";
+  os << "\n  tiles: " << t.num_tiles << ", smem/CTA: " << t.smem_bytes
+     << " B, tables: " << t.table_bytes << " B\n";
   return os.str();
 }
 

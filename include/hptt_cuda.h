@@ -172,25 +172,29 @@ int hptt_cuda_debug_check_indexing(int dtype, uint32_t rank, const uint32_t *in_
  *
  * No counterpart in the reference.  hptt_cuda_plan_create keeps a plan's
  * offset tables (a few KB) in device memory it obtains with cudaMalloc.
- * Callers that cannot allocate device memory when they transpose -- code
- * recording work while a stream is being captured, frameworks whose device
- * memory comes only from their own pool or arena, jobs held to a fixed
- * memory budget -- use this call instead.  It plans the transpose on the
- * host, copies the tables into a fixed HPTT_NOALLOC_TABLE_BYTES array
- * compiled into the library, and enqueues the same kernel on `stream`
- * (cudaStream_t as void*, NULL = the legacy default stream).  It never calls
- * cudaMalloc, cudaFree or another device allocator.
+ * Callers that cannot allocate device memory when they transpose --
+ * frameworks whose device memory comes only from their own pool or arena
+ * (an allocation behind the pool's back breaks its accounting or fails under
+ * its reservation), jobs held to a fixed device-memory budget -- use this
+ * call instead.  It plans the transpose on the host (with the autotune
+ * cache's entry for the problem when there is one), copies the tables into
+ * a fixed HPTT_NOALLOC_TABLE_BYTES array compiled into the library, and
+ * enqueues the same kernel on `stream` (cudaStream_t as void*, NULL = the
+ * legacy default stream).  It never calls cudaMalloc, cudaFree or another
+ * device allocator.  The table copy is a cudaMemcpyAsync from pageable host
+ * memory that the call owns and frees before it returns.
  *
  * Arguments mean what they mean for hptt_cuda_plan_create; in/out are device
- * pointers the caller owns.  Returns HPTT_ERR_TOO_LARGE when this problem's
- * tables would not fit the array.
+ * pointers the caller owns.  Returns HPTT_ERR_TOO_LARGE, before any copy or
+ * launch, when this problem's tables would not fit the array.
  *
  * The array is shared by every call in the process on that GPU and keeps
  * the last call's tables: calls that can run at the same time on the GPU
  * (different streams, several host threads) race on it and must be
  * serialised by the caller; calls on one stream are ordered.  The first call
- * on each device looks the array's address up (a one-time set-up); make
- * that first call before any stream capture begins.
+ * on each device looks the array's address up (a one-time set-up, kept for
+ * the life of the process; after cudaDeviceReset the call must not be used
+ * again in that process).
  */
 int hptt_cuda_transpose_noalloc(int dtype, uint32_t rank, const uint32_t *in_size,
                                 const uint32_t *perm, const uint32_t *in_outer,

@@ -32,13 +32,21 @@ _u32p = ctypes.POINTER(ctypes.c_uint32)
 _dp = ctypes.POINTER(ctypes.c_double)
 
 
+def ref_dir() -> str | None:
+    """The reference checkout named by HPTT_REF_DIR, when its sources exist."""
+    d = os.environ.get("HPTT_REF_DIR", "")
+    return d if d and os.path.isdir(os.path.join(d, "src")) else None
+
+
 def build(with_ref: bool | None = None) -> None:
-    """Compile liboracle.so (and the reference library when its sources exist)."""
+    """Compile liboracle.so, and the reference library from the checkout that
+    HPTT_REF_DIR names (with_ref None: when that checkout exists)."""
     subprocess.run(["make", "-s", "-C", HERE, "all"], check=True)
     if with_ref is None:
-        with_ref = os.path.isdir("/root/reference/src")
+        with_ref = ref_dir() is not None
     if with_ref:
-        subprocess.run(["make", "-s", "-j8", "-C", HERE, "ref"], check=True)
+        subprocess.run(["make", "-s", "-j8", "-C", HERE, "ref", f"REF={ref_dir() or ''}"],
+                       check=True)
 
 
 _oracle = None

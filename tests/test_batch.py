@@ -188,3 +188,70 @@ def test_empty_batch():
     assert b.info() == (0, 0, 0)
     b.exec()
     b.destroy()
+
+
+@pytest.mark.gpu
+def test_batch_benchmark_sizes_against_oracle():
+    """A quarter of the benchmark's 4096-transpose mixed workload (every
+    fourth entry: 1024 transposes of 4 KB - 16 MB each, all four element
+    types, ranks 2-6, half alpha=1/beta=0, complex scalars for complex types)
+    at its own sizes and with the shipped tuned tiles, run as one batch: every
+    entry compared with the oracle bit for bit, and the batch uses as many
+    group kernels (tile bodies) as the whole workload does."""
+    import os
+    import oracle
+    from hptt_b200.workloads import batch_cases
+    torch = _torch()
+    path = os.path.join(os.path.dirname(h.__file__), "tune", "b200.cache")
+    h.tune_cache_clear()
+    if os.path.exists(path):
+        h.tune_cache_load(path)
+    try:
+        allc = batch_cases()
+        # group kernels of the whole workload: plans only record pointers, so
+        # one scratch buffer of the largest footprint stands in for every
+        # tensor (nothing is launched on it)
+        biggest = max(int(np.prod(c["in_size"])) * {"f32": 4, "f64": 8, "c64": 8,
+                                                   "c128": 16}[c["dtype"]] for c in allc)
+        scratch = torch.empty(biggest, dtype=torch.uint8, device="cuda")
+        dry = [h.create_plan(scratch, scratch, c["in_size"], c["perm"], c["alpha"], c["beta"],
+                             0, dtype=c["dtype"]) for c in allc]
+        full_kernels = h.create_batch(dry).info()[2]
+        del dry
+        cases = allc[::4]
+        g = torch.Generator(device="cuda").manual_seed(44)
+        ents = []
+        for c in cases:
+            n = int(np.prod(c["in_size"]))
+            t = _tdt(torch, c["dtype"])
+            if c["dtype"] in ("c64", "c128"):
+                rt = torch.float32 if c["dtype"] == "c64" else torch.float64
+                da = torch.view_as_complex(torch.rand(n, 2, generator=g, device="cuda", dtype=rt) * 2 - 1)
+                db = torch.view_as_complex(torch.rand(n, 2, generator=g, device="cuda", dtype=rt) * 2 - 1)
+            else:
+                da = torch.rand(n, generator=g, device="cuda", dtype=t) * 2 - 1
+                db = torch.rand(n, generator=g, device="cuda", dtype=t) * 2 - 1
+            b0 = db.cpu().numpy()
+            p = h.create_plan(da, db, c["in_size"], c["perm"], c["alpha"], c["beta"], 0,
+                              dtype=c["dtype"])
+            assert p is not None
+            ents.append((c, da, db, b0, p))
+        batch = h.create_batch([e[4] for e in ents])
+        nbytes, items, kernels = batch.info()
+        assert kernels == full_kernels, (kernels, full_kernels)
+        batch.exec()
+        torch.cuda.synchronize()
+        for c, da, db, b0, p in ents:
+            a = oracle.aligned_empty(da.numel(), oracle.NP_DTYPES[c["dtype"]])
+            a[:] = da.cpu().numpy()
+            b0a = oracle.aligned_empty(b0.size, b0.dtype)
+            b0a[:] = b0
+            cs = isinstance(c["alpha"], complex) or isinstance(c["beta"], complex)
+            want = oracle_run(c["dtype"], c["in_size"], c["perm"], c["alpha"], c["beta"], a,
+                              b0a, complex_scalars=cs)
+            assert_same(db.cpu().numpy(), want, c["dtype"],
+                        f"batch entry {c['dtype']} {c['in_size']} {c['perm']} "
+                        f"a={c['alpha']} b={c['beta']}")
+        batch.destroy()
+    finally:
+        h.tune_cache_clear()

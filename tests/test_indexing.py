@@ -79,3 +79,45 @@ def test_replay_shapes(dt, size, perm):
         rc, n = check(dt, size, perm, max_vec_bytes=mv)
         assert rc == 0, (dt, size, perm, mv, rc)
         assert n == np.prod(size)
+
+
+# Ranks 7 and 8 (the reference generates them when built with a larger
+# HPTT_CODE_GEN_TRANS_ORDER_MAX, README.md:38-46).  No two neighbouring output
+# dims are consecutive input dims in order, so nothing fuses below rank 7.
+HIGH_RANK = [
+    ("f32", [3, 4, 2, 5, 3, 2, 4], [6, 4, 2, 0, 5, 3, 1]),
+    ("f64", [5, 3, 7, 2, 4, 3, 6], [3, 0, 6, 2, 5, 1, 4]),
+    ("c64", [2, 3, 4, 2, 3, 2, 5, 3], [7, 5, 3, 1, 6, 4, 2, 0]),
+    ("c128", [5, 7, 3, 4, 6, 3, 2, 5], [1, 5, 0, 7, 3, 6, 2, 4]),
+    ("f32", [33, 2, 3, 4, 2, 3, 2, 17], [0, 5, 2, 7, 4, 1, 6, 3]),
+    ("f64", [9, 4, 3, 2, 5, 2, 3, 11], [7, 2, 5, 0, 3, 6, 1, 4]),
+]
+
+
+def fused_rank(dt, size, perm):
+    d = h.inspect_plan(dt, size, perm)
+    return int(d.split("fused rank:")[1].split()[0])
+
+
+@pytest.mark.parametrize("dt,size,perm", HIGH_RANK)
+def test_replay_ranks_7_and_8(dt, size, perm):
+    assert fused_rank(dt, size, perm) == len(size)
+    for mv in (0, {"f32": 4, "f64": 8, "c64": 8, "c128": 16}[dt]):
+        rc, n = check(dt, size, perm, max_vec_bytes=mv)
+        assert rc == 0, (dt, size, perm, mv, rc)
+        assert n == np.prod(size)
+
+
+@pytest.mark.parametrize("seed", range(60))
+def test_replay_random_ranks_7_and_8(seed):
+    rng = np.random.default_rng(5000 + seed)
+    rank = 7 + seed % 2
+    dt = ["f32", "f64", "c64", "c128"][seed % 4]
+    size = [int(x) for x in np.exp(rng.uniform(np.log(2), np.log(12), rank)).astype(int)]
+    while np.prod(size) > 300000:
+        size[int(np.argmax(size))] //= 2
+    size = [max(2, s) for s in size]
+    perm = [int(x) for x in rng.permutation(rank)]
+    rc, n = check(dt, size, perm)
+    assert rc == 0, (dt, size, perm, rc)
+    assert n == np.prod(size)

@@ -1,12 +1,12 @@
 """The allocation-free entry point, hptt_cuda_transpose_noalloc.
 
 Some callers cannot allocate device memory at the moment they transpose:
-code recording work while a stream is captured, frameworks that hand out
-device memory only from their own pool, jobs held to a fixed budget.  For
-them the offset tables go into a fixed array compiled into the library
-instead of a cudaMalloc'd buffer.  Its results must equal those of the
-plan-based entry point (hptt_cuda_plan_create + hptt_cuda_plan_exec) bit for
-bit, also on consecutive calls that reuse the shared array.
+frameworks that hand out device memory only from their own pool or arena,
+jobs held to a fixed device-memory budget.  For them the offset tables go
+into a fixed array compiled into the library instead of a cudaMalloc'd
+buffer.  Its results must equal those of the plan-based entry point
+(hptt_cuda_plan_create + hptt_cuda_plan_exec) and of the oracle bit for bit,
+also on consecutive calls that reuse the shared array.
 
 The file name makes pytest collect it last, so a run that stops at its first
 failure has already run every other test.
@@ -16,7 +16,7 @@ import ctypes
 import numpy as np
 import pytest
 
-from helpers import assert_same, footprint, gpu_run, seeded
+from helpers import assert_same, footprint, gpu_run, oracle_run, seeded
 
 pytestmark = pytest.mark.gpu
 
@@ -78,6 +78,8 @@ def test_noalloc_matches_plan_twice(case):
         want = gpu_run(name, size, perm, al, be, a, b0, io, oo, complex_scalars=cs)
         got = _run_noalloc(name, size, perm, al, be, a, b0, io, oo, cs)
         assert_same(got, want, name, f"no-alloc call {call}")
+        ref = oracle_run(name, size, perm, al, be, a, b0, io, oo, complex_scalars=cs)
+        assert_same(got, ref, name, f"no-alloc call {call} vs oracle")
 
 
 def test_noalloc_alternating_shapes():
@@ -90,6 +92,8 @@ def test_noalloc_alternating_shapes():
         want = gpu_run(name, size, perm, 2.3, 4.2, a, b0)
         got = _run_noalloc(name, size, perm, 2.3, 4.2, a, b0)
         assert_same(got, want, name, f"alternating {size}")
+        assert_same(got, oracle_run(name, size, perm, 2.3, 4.2, a, b0), name,
+                    f"alternating {size} vs oracle")
 
 
 def test_noalloc_rejects_bad_arguments():
