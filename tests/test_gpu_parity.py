@@ -252,6 +252,11 @@ FORM_SHAPES = [
     ("f32", [49, 88, 93, 6], [1, 3, 0, 2]),
     ("c64", [12, 4, 4, 11, 19, 13], [4, 0, 5, 3, 1, 2]),
     ("c128", [6, 6, 15, 77, 6, 3], [1, 2, 5, 0, 3, 4]),
+    ("f64", [37, 29, 23], [2, 1, 0]),
+    ("c128", [33, 17, 5], [1, 0, 2]),
+    ("c64", [70, 41], [1, 0]),
+    ("f32", [300, 7, 13], [2, 0, 1]),
+    ("f32", [1000, 333], [1, 0]),
 ]
 
 

@@ -33,7 +33,7 @@ def _random_case(seed):
     rank = int(rng.integers(2, 7))
     dt = ["f32", "f64", "c64", "c128"][int(rng.integers(0, 4))]
     size = [int(x) for x in np.exp(rng.uniform(0, np.log(40), rank)).astype(int) + 1]
-    while np.prod(size) > 200000:
+    while np.prod(size) > 80000:
         size[int(np.argmax(size))] //= 2
     perm = [int(x) for x in rng.permutation(rank)]
     io = oo = None
@@ -75,7 +75,8 @@ SHAPES = [
 
 @pytest.mark.parametrize("dt,size,perm", SHAPES)
 def test_replay_shapes(dt, size, perm):
-    for mv in (0, 4):
+    # the vector limit only changes row-kernel plans (shared stride-1 dim)
+    for mv in ((0, 4) if perm[0] == 0 else (0,)):
         rc, n = check(dt, size, perm, max_vec_bytes=mv)
         assert rc == 0, (dt, size, perm, mv, rc)
         assert n == np.prod(size)
