@@ -22,10 +22,16 @@ roofline  = the dominant kernel's achieved bandwidth over the measured HBM
 tiles     = from the shipped autotune cache (hptt_b200/tune/b200.cache, made
             on a B200 by `python -m hptt_b200.tune_sweep`); a shape it does
             not hold uses the planner's heuristic (--no-tune-cache: always)
-cpu_baseline = the reference's own CPU plan (oracle/_ref, built from the
+cpu_baseline = the reference's own CPU code (oracle/_ref, built from the
             reference sources) on a bounded sample of the same workload, all
-            host threads; shapes where the reference plan is incorrect are
-            timed with the reference's naive RefTrans instead, labelled.
+            host threads: its plan where that plan is correct for the shape,
+            else its naive RefTrans, labelled.
+plain     = config 1 (f32 {256,256,256}, perm {2,1,0}, alpha 2.3, beta 4.2):
+            device GB/s with L2 flushed before every timed launch, roofline,
+            e2e, and the reference plan at 1 thread and at all host threads
+hard      = config 3 (c64/c128 rank-6 hard layouts, complex scalars): device
+            GB/s, roofline, e2e, the reference's naive transpose on the host
+            (complex scalars are not expressible through the reference API)
 
 served   = the served form: Poisson arrivals over the same 4096 plans at
             10k-500k requests/s (2 s windows by default, --serve-seconds 60
@@ -38,7 +44,8 @@ batched  = the batched form on the 4096-transpose mixed workload: one graph
 
 N > 1 (torchrun): every rank runs the whole workload on its own GPU
 (independent transposes; no collective on the data path), scaling "weak".
-`--impl reference` times only the reference's CPU implementation (rank 0).
+`--impl reference` times only the reference's CPU implementation (rank 0):
+every step the whole workload (all 96 sweep transposes), all host threads.
 """
 from __future__ import annotations
 
@@ -162,25 +169,12 @@ def _tdtype(torch, name):
             "c128": torch.complex128}[name]
 
 
-def run_ours(args, rank, world, dist):
+def _make_plans(cases, rank):
+    """Resident buffers (one A and one B per distinct tensor shape) and one
+    plan per transpose; seeded uniform[-1, 1] data made on the device."""
     import torch
     import hptt_b200 as h
     from hptt_b200.workloads import algorithmic_bytes
-
-    dev = int(os.environ.get("LOCAL_RANK", "0"))
-    torch.cuda.set_device(dev)
-    cases, desc = _workload(args.workload)
-    if args.case is not None:
-        cases = [cases[args.case]]
-        desc += f" -- transpose {args.case} only"
-    stream = torch.cuda.current_stream()
-    tiles = "planner heuristic"
-    if not args.no_tune_cache and args.tune_cache and os.path.exists(args.tune_cache):
-        h.tune_cache_load(args.tune_cache)
-        tiles = (f"autotune cache {os.path.relpath(args.tune_cache, ROOT)} "
-                 f"({h.tune_cache_size()} entries; heuristic on a miss)")
-
-    # resident buffers: one A and one B per distinct tensor shape
     bufs = {}
     plans = []
     g = torch.Generator(device="cuda").manual_seed(1234 + rank)
@@ -204,86 +198,178 @@ def run_ours(args, rank, world, dist):
         kind = "rows" if "kernel: rows" in p.describe() else "tile"
         plans.append((p, algorithmic_bytes(c), kind, c))
     torch.cuda.synchronize()
+    return plans, bufs
+
+
+def _timed_steps(plans, steps, warmup, stream, dist, world, flush=None):
+    """Warm-up, then `steps` timed steps (every transpose once per step) with
+    a CUDA event pair around every launch.  Returns the max-over-ranks device
+    time of the steps (ms), each plan's summed per-launch time (ms), and the
+    clock samples.  flush: an L2 flush run before every launch, outside the
+    per-launch events (the step time then counts per-launch times only)."""
+    import torch
     sptr = stream.cuda_stream
 
     def step(record=None):
         for i, (p, _, _, _) in enumerate(plans):
+            if flush is not None:
+                flush()
             if record is not None:
                 record[i][0].record(stream)
             p.exec_on(sptr)
             if record is not None:
                 record[i][1].record(stream)
 
-    for _ in range(args.warmup):
+    for _ in range(warmup):
         step()
     torch.cuda.synchronize()
     if world > 1:
         dist.barrier()
-    sampler = ClockSampler(dev)
+    sampler = ClockSampler(int(os.environ.get("LOCAL_RANK", "0")))
     sampler.start()
     ev = [[(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
-           for _ in plans] for _ in range(args.steps)]
+           for _ in plans] for _ in range(steps)]
     t0 = torch.cuda.Event(enable_timing=True)
     t1 = torch.cuda.Event(enable_timing=True)
     torch.cuda.synchronize()
     t0.record(stream)
-    for k in range(args.steps):
+    for k in range(steps):
         step(ev[k])
     t1.record(stream)
     torch.cuda.synchronize()
     clocks = sampler.stop()
-    elapsed_ms = t0.elapsed_time(t1)
-    per_launch_ms = [sum(ev[k][i][0].elapsed_time(ev[k][i][1]) for k in range(args.steps))
+    per_launch_ms = [sum(ev[k][i][0].elapsed_time(ev[k][i][1]) for k in range(steps))
                      for i in range(len(plans))]
+    elapsed_ms = sum(per_launch_ms) if flush is not None else t0.elapsed_time(t1)
     elapsed_ms = max_over_ranks(elapsed_ms, dist, world)
-    device_ms = sum(per_launch_ms)
+    return elapsed_ms, per_launch_ms, clocks
 
-    bytes_step = sum(bb for _, bb, _, _ in plans)
-    value = aggregate_gbs(bytes_step * args.steps, world, elapsed_ms)
-    ms_per_step = elapsed_ms / args.steps
 
-    # dominant kernel: the kernel kind with the most device time
+def _roofline(plans, per_launch_ms, steps, traffic_ratio=None):
+    """The dominant kernel kind (most device time): its algorithmic bytes per
+    launch over its average launch duration, against the measured peak."""
     by_kind = {}
     for (p, bb, kind, _), ms in zip(plans, per_launch_ms):
         d = by_kind.setdefault(kind, [0.0, 0, 0])
         d[0] += ms
-        d[1] += bb * args.steps
-        d[2] += args.steps
+        d[1] += bb * steps
+        d[2] += steps
+    device_ms = sum(per_launch_ms)
     dom = max(by_kind, key=lambda k: by_kind[k][0])
     dom_ms, dom_bytes, dom_launches = by_kind[dom]
     peak, peak_kind = _peaks()
     achieved = dom_bytes / (dom_ms / 1e3) / 1e9
-    # the committed launch list covers the full sweep step
-    traffic = _profiled_traffic(dom) if args.workload == "sweep" and args.case is None else None
-    roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak,
-                "unit": "GB/s", "frac": round(achieved / peak, 4),
-                "traffic": traffic, "kernel": "k_tile" if dom == "tile" else "k_rows",
-                "peak_source": ("measured (MEASURED_PEAKS.json hbm_gbs, burst copy)"
-                                if peak_kind == "measured" else
-                                "fallback 6650 GB/s (MEASURED_PEAKS.json absent)"),
-                "launches": dom_launches,
-                "algorithmic_bytes_per_launch": int(dom_bytes // max(1, dom_launches)),
-                "share_of_device_time": round(dom_ms / device_ms, 4)}
+    per_launch = int(dom_bytes // max(1, dom_launches))
+    return {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak,
+            "unit": "GB/s", "frac": round(achieved / peak, 4),
+            "traffic": int(per_launch * traffic_ratio) if traffic_ratio else None,
+            "kernel": "k_tile" if dom == "tile" else "k_rows",
+            "peak_source": ("measured (MEASURED_PEAKS.json hbm_gbs, burst copy)"
+                            if peak_kind == "measured" else
+                            "fallback 6650 GB/s (MEASURED_PEAKS.json absent)"),
+            "launches": dom_launches,
+            "algorithmic_bytes_per_launch": per_launch,
+            "share_of_device_time": round(dom_ms / device_ms, 4)}
+
+
+def _l2_flush():
+    """A callable that overwrites a 256 MB device buffer (twice the L2)."""
+    import torch
+    junk = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    return lambda: junk.fill_(1)
+
+
+def run_section(args, name, stream):
+    """One more workload measured the way the sweep is: device GB/s with the
+    dominant kernel's roofline, the end-to-end figure through the C ABI with
+    host buffers, and the reference's CPU code on the same cases.  The plain
+    single transpose (64 MB tensors: A and B together about the size of L2)
+    flushes L2 before every timed launch; the hard layouts (~256 MB tensors)
+    need no flush."""
+    cases, desc = _workload(name)
+    plans, bufs = _make_plans(cases, 0)
+    flush = _l2_flush() if name == "plain" else None
+    steps = 50 if name == "plain" else 20
+    ms, per_launch, clocks = _timed_steps(plans, steps, 3, stream, None, 1, flush=flush)
+    bytes_step = sum(bb for _, bb, _, _ in plans)
+    peak, _ = _peaks()
+    value = bytes_step * steps / (ms / 1e3) / 1e9
+    out = {"workload": desc, "transposes_per_step": len(plans), "bytes_per_step": bytes_step,
+           "steps": steps, "value": round(value, 1), "unit": "GB/s",
+           "ms_per_step": round(ms / steps, 4), "hbm_frac": round(value / peak, 4),
+           "l2": ("L2 flushed (256 MB write) before every timed launch; per-launch events"
+                  if flush is not None else "inputs larger than L2 (no flush)"),
+           "roofline": _roofline(plans, per_launch, steps),
+           "e2e": (run_e2e(args, plans, bufs, stream, e2e_steps=max(args.e2e_steps, 24 // len(plans)))
+                   if args.e2e_steps > 0 else None),
+           "clocks": clocks}
+    if not args.no_cpu_baseline:
+        out["cpu_baseline"] = (cpu_baseline_plain() if name == "plain"
+                               else cpu_baseline_sample(cases, budget_s=args.cpu_budget))
+    for p, _, _, _ in plans:
+        p.destroy()
+    del bufs
+    return out
+
+
+def run_ours(args, rank, world, dist):
+    import torch
+    import hptt_b200 as h
+
+    dev = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(dev)
+    cases, desc = _workload(args.workload)
+    if args.case is not None:
+        cases = [cases[args.case]]
+        desc += f" -- transpose {args.case} only"
+    stream = torch.cuda.current_stream()
+    tiles = "planner heuristic"
+    if not args.no_tune_cache and args.tune_cache and os.path.exists(args.tune_cache):
+        h.tune_cache_load(args.tune_cache)
+        tiles = (f"autotune cache {os.path.relpath(args.tune_cache, ROOT)} "
+                 f"({h.tune_cache_size()} entries; heuristic on a miss)")
+
+    plans, bufs = _make_plans(cases, rank)
+    flush = _l2_flush() if args.workload == "plain" else None
+    elapsed_ms, per_launch_ms, clocks = _timed_steps(plans, args.steps, args.warmup, stream,
+                                                     dist, world, flush=flush)
+    device_ms = sum(per_launch_ms)
+    bytes_step = sum(bb for _, bb, _, _ in plans)
+    value = aggregate_gbs(bytes_step * args.steps, world, elapsed_ms)
+    ms_per_step = elapsed_ms / args.steps
+    peak, _ = _peaks()
+    # DRAM traffic per launch: the committed per-case ncu captures of the
+    # sweep (profiles/traffic.json), as a ratio to algorithmic bytes
+    ratio = _profiled_traffic() if args.workload == "sweep" and args.case is None else None
+    roofline = _roofline(plans, per_launch_ms, args.steps, ratio)
 
     e2e = run_e2e(args, plans, bufs, stream, dist, world) if args.e2e_steps > 0 else None
-    # the batched and served forms are measured on one GPU (N > 1 runs
-    # replicas of the sweep only)
-    batched = served = None
-    if world == 1 and args.case is None and not (args.no_batched and args.no_served):
+    gpu_launches = sum(p.launches for p, _, _, _ in plans) * args.steps
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline_sample(cases, budget_s=args.cpu_budget)
+    for p, _, _, _ in plans:
+        p.destroy()
+    del bufs
+    torch.cuda.synchronize()
+    torch.cuda.empty_cache()
+    # the batched and served forms and the other configurations are measured
+    # on one GPU (N > 1 runs replicas of the sweep only)
+    batched = served = contraction = plain = hard = None
+    single = world == 1 and args.case is None and args.workload == "sweep"
+    if single and not args.no_sections:
+        plain = run_section(args, "plain", stream)
+        hard = run_section(args, "hard", stream)
+        torch.cuda.empty_cache()
+    if single and not (args.no_batched and args.no_served):
         pool, pool_buffers = _batch_pool(args)
         if not args.no_batched:
             batched = run_batched(args, stream, pool)
         if not args.no_served:
             served = run_served(args, pool)
         del pool, pool_buffers
-    contraction = None
-    if world == 1 and args.case is None and not args.no_contraction:
+    if single and not args.no_contraction:
         contraction = run_contractions(args)
-    gpu_launches = sum(p.launches for p, _, _, _ in plans) * args.steps
-
-    cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu = cpu_baseline_sample(cases, budget_s=args.cpu_budget)
 
     out = {
         "metric": METRIC, "value": round(value, 1), "unit": "GB/s", "n_gpus": world,
@@ -292,7 +378,9 @@ def run_ours(args, rank, world, dist):
         "dtype": "f32+f64" if args.workload == "sweep" else cases[0]["dtype"],
         "data": "synthetic (seeded uniform[-1,1]; shapes from the workload generator)",
         "config": {"workload": desc, "transposes_per_step": len(plans),
-                   "bytes_per_step": bytes_step, "l2": "inputs larger than L2 (no flush)",
+                   "bytes_per_step": bytes_step,
+                   "l2": ("L2 flushed (256 MB write) before every timed launch"
+                          if flush is not None else "inputs larger than L2 (no flush)"),
                    "tiles": tiles,
                    "parallelism": f"replicas x{world}"},
         "hbm_frac": round(value / world / peak, 4),
@@ -301,6 +389,8 @@ def run_ours(args, rank, world, dist):
         "gpu_launches": gpu_launches,
         "clocks": clocks,
         "cpu_baseline": cpu,
+        "plain": plain,
+        "hard": hard,
         "batched": batched,
         "served": served,
         "contraction": contraction,
@@ -309,21 +399,20 @@ def run_ours(args, rank, world, dist):
     return out
 
 
-def _profiled_traffic(kind):
-    """DRAM bytes (read + write) per launch of the dominant kernel, averaged
-    over its launches in one step of the sweep, from the committed ncu launch
-    list (profiles/traffic.json; see profiles/k_tile_sweep_launches.md)."""
+def _profiled_traffic():
+    """DRAM bytes (read + write) per algorithmic byte of the sweep's tile
+    launches, from the committed one-launch ncu captures of sample cases
+    (profiles/traffic.json; see profiles/k_tile_sweep_traffic.md)."""
     p = os.path.join(ROOT, "profiles", "traffic.json")
     if not os.path.exists(p):
         return None
     try:
-        d = json.load(open(p)).get(kind)
-        return int(d["dram_bytes_per_launch"]) if d else None
+        return float(json.load(open(p))["dram_per_algorithmic_byte"])
     except Exception:
         return None
 
 
-def run_e2e(args, plans, bufs, stream, dist=None, world=1):
+def run_e2e(args, plans, bufs, stream, dist=None, world=1, e2e_steps=None):
     """Same workload through the C ABI with host buffers, copies timed.
 
     Every transpose copies its A (and B when B is read) from pinned host
@@ -387,13 +476,14 @@ def run_e2e(args, plans, bufs, stream, dist=None, world=1):
         torch.cuda.synchronize()
         return e0.elapsed_time(e1)
 
+    nsteps = e2e_steps or args.e2e_steps
     timed(1)  # warm-up
-    ms = timed(args.e2e_steps)
+    ms = timed(nsteps)
     ms = max_over_ranks(ms, dist, world)
-    total = sum(bb for _, bb, _, _ in plans) * args.e2e_steps
+    total = sum(bb for _, bb, _, _ in plans) * nsteps
     return {"value": round(aggregate_gbs(total, world, ms), 2), "unit": "GB/s",
             "h2d_bytes_per_step": h2d * world, "d2h_bytes_per_step": d2h * world,
-            "steps": args.e2e_steps, "ms_per_step": round(ms / args.e2e_steps, 3),
+            "steps": nsteps, "ms_per_step": round(ms / nsteps, 3),
             "api": "TransPlan.reset_data + exec_on (C ABI) with pinned host<->device "
                    "copies, three streams"}
 
@@ -647,15 +737,35 @@ def _fill(x: np.ndarray, seed: int):
     flat[:] = np.tile(blk.astype(flat.dtype), reps)[:flat.size]
 
 
-def reference_time_case(c, threads, repeat=2):
-    """Best-of-`repeat` time of one case on the reference's CPU code."""
+class _HostBuffers:
+    """One page-aligned A/B pair of the largest footprint a workload needs,
+    filled once; every case runs on leading views of it (the reference's CPU
+    time depends on the shape, not on the values)."""
+
+    def __init__(self, cases):
+        import oracle
+        from hptt_b200.workloads import ELEM
+        nbytes = max(int(np.prod(c["in_size"])) * ELEM[c["dtype"]] for c in cases)
+        n = (nbytes + 15) // 16 * 2  # float64 words, a whole number of 16-byte elements
+        self.a = oracle.aligned_empty(n, np.float64)
+        self.b = oracle.aligned_empty(n, np.float64)
+        _fill(self.a, 1)
+        _fill(self.b, 2)
+
+    def views(self, c):
+        import oracle
+        dt = oracle.NP_DTYPES[c["dtype"]]
+        n = int(np.prod(c["in_size"]))
+        return self.a.view(dt)[:n], self.b.view(dt)[:n]
+
+
+def reference_time_case(c, threads, repeat=2, bufs=None):
+    """Best-of-`repeat` time of one case on the reference's CPU code: its
+    optimised plan where that plan is correct for the shape, else its naive
+    RefTrans (labelled "naive")."""
     import oracle
     name = c["dtype"]
-    n = int(np.prod(c["in_size"]))
-    a = oracle.aligned_empty(n, oracle.NP_DTYPES[name])
-    b = oracle.aligned_empty(n, oracle.NP_DTYPES[name])
-    _fill(a, 1)
-    _fill(b, 2)
+    a, b = (bufs or _HostBuffers([c])).views(c)
     al, be = c["alpha"], c["beta"]
     if isinstance(al, complex) or isinstance(be, complex):
         # complex scalars are not expressible through the reference API: time
@@ -672,13 +782,23 @@ def reference_time_case(c, threads, repeat=2):
     return t, "naive"
 
 
-def cpu_baseline_sample(cases, budget_s=20.0, threads=None):
+def _ref_ready():
     import oracle
+    if not oracle.ref_available():
+        return "oracle/_ref/libhptt_ref.so not built"
+    if not _host_has_avx2():
+        return "host CPU lacks AVX2 (reference AVX2 build)"
+    return None
+
+
+def cpu_baseline_sample(cases, budget_s=20.0, threads=None):
     from hptt_b200.workloads import algorithmic_bytes
-    if not oracle.ref_available() or not _host_has_avx2():
+    why = _ref_ready()
+    if why:
         return {"value": None, "unit": "GB/s", "cores": 0, "kind": "reference",
-                "sample": "unavailable: reference library not built or host lacks AVX2"}
+                "sample": "unavailable: " + why}
     threads = threads or os.cpu_count() or 1
+    bufs = _HostBuffers(cases)
     t_start = time.time()
     tot_b = tot_t = 0.0
     used = {"plan": 0, "naive": 0}
@@ -687,7 +807,7 @@ def cpu_baseline_sample(cases, budget_s=20.0, threads=None):
     for i in order:
         if time.time() - t_start > budget_s:
             break
-        t, how = reference_time_case(cases[i], threads)
+        t, how = reference_time_case(cases[i], threads, bufs=bufs)
         tot_b += algorithmic_bytes(cases[i])
         tot_t += t
         used[how] += 1
@@ -700,40 +820,84 @@ def cpu_baseline_sample(cases, budget_s=20.0, threads=None):
                        f"those shapes or complex scalars)")}
 
 
-def run_reference(args):
+def cpu_baseline_plain(runs=5):
+    """The plain single transpose on the reference's own optimised CPU plan
+    (inc/hptt/cgraph/cgraph_trans.tcc:27-48; the shape is in the subset where
+    that plan is correct) at 1 OpenMP thread and at every host thread: best
+    of `runs` execs, an 800 MB host buffer rewritten between execs so no run
+    starts with the tensors in cache."""
     import oracle
+    from hptt_b200.workloads import algorithmic_bytes, plain_single
+    why = _ref_ready()
+    if why:
+        return {"value": None, "unit": "GB/s", "cores": 0, "kind": "reference",
+                "sample": "unavailable: " + why}
+    c = plain_single()
+    assert oracle.ref_plan_is_safe(c["dtype"], c["in_size"], c["perm"], c["beta"])
+    bufs = _HostBuffers([c])
+    a, b = bufs.views(c)
+    trash = np.empty(100 << 20, dtype=np.float64)
+    nb = algorithmic_bytes(c)
+    res = {}
+    for threads in (1, os.cpu_count() or 1):
+        best = 1e30
+        for r in range(runs):
+            trash.fill(float(r))
+            best = min(best, oracle.ref_plan_exec(a, b, c["in_size"], c["perm"], c["alpha"],
+                                                  c["beta"], threads=threads, repeat=1))
+        res[threads] = nb / best / 1e9
+    allc = os.cpu_count() or 1
+    return {"value": round(res[allc], 2), "unit": "GB/s", "cores": allc, "kind": "reference",
+            "value_1_thread": round(res[1], 2),
+            "sample": (f"the whole transpose on the reference plan, best of {runs} execs with "
+                       f"an 800 MB cache rewrite between execs, at 1 and {allc} OpenMP threads")}
+
+
+def run_reference(args):
+    """The reference arm: the reference's own CPU code (its plan where it is
+    correct for the shape, else its naive RefTrans, labelled) on every
+    transpose of the workload, each step the whole workload, all host
+    threads.  Steps past a time budget are not run (the line says how many
+    were timed)."""
     from hptt_b200.workloads import algorithmic_bytes
     cases, desc = _workload(args.workload)
     threads = os.cpu_count() or 1
-    if not oracle.ref_available():
-        return {"impl": "reference", "unavailable": "oracle/_ref/libhptt_ref.so not built"}
-    if not _host_has_avx2():
-        return {"impl": "reference", "unavailable": "host CPU lacks AVX2 (reference AVX2 build)"}
-    # each step: a rotating sample of cases (bounded CPU time)
-    per_step = max(1, min(len(cases), args.ref_cases_per_step))
+    why = _ref_ready()
+    if why:
+        return {"impl": "reference", "unavailable": why}
+    bufs = _HostBuffers(cases)
     tot_b = tot_t = 0.0
     used = {"plan": 0, "naive": 0}
-    idx = 0
+    timed = 0
+    t_start = time.time()
     for s in range(args.warmup + args.steps):
-        for _ in range(per_step):
-            c = cases[idx % len(cases)]
-            idx += 1
-            t, how = reference_time_case(c, threads, repeat=1)
+        if s >= args.warmup and timed and time.time() - t_start > args.ref_budget:
+            break
+        step_b = step_t = 0.0
+        for c in cases:
+            t, how = reference_time_case(c, threads, repeat=1, bufs=bufs)
+            step_b += algorithmic_bytes(c)
+            step_t += t
             if s >= args.warmup:
-                tot_b += algorithmic_bytes(c)
-                tot_t += t
                 used[how] += 1
+        if s >= args.warmup:
+            tot_b += step_b
+            tot_t += step_t
+            timed += 1
     value = tot_b / tot_t / 1e9 if tot_t else None
-    sample = (f"{per_step} transposes per step (rotating through the workload), "
-              f"{used['plan']} by the reference plan, {used['naive']} by the reference's "
-              f"naive RefTrans (plan incorrect on those shapes)")
+    sample = (f"every step the whole workload ({len(cases)} transposes; {timed} timed steps "
+              f"after {args.warmup} warm-up), {threads} OpenMP threads; per step "
+              f"{used['plan'] // max(1, timed)} transposes by the reference plan and "
+              f"{used['naive'] // max(1, timed)} by the reference's naive RefTrans (plan "
+              f"incorrect on those shapes, or complex scalars)")
     return {
         "impl": "reference", "metric": METRIC, "value": round(value, 2) if value else None,
-        "unit": "GB/s", "n_gpus": 0, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": round(tot_t * 1e3 / max(1, args.steps), 3),
+        "unit": "GB/s", "n_gpus": 0, "steps": timed, "warmup": args.warmup,
+        "ms_per_step": round(tot_t * 1e3 / max(1, timed), 3),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32+f64" if args.workload == "sweep" else cases[0]["dtype"],
-        "data": "synthetic", "config": {"workload": desc, "threads": threads},
+        "data": "synthetic", "config": {"workload": desc, "threads": threads,
+                                        "transposes_per_step": len(cases)},
         "cpu_baseline": {"value": round(value, 2) if value else None, "unit": "GB/s",
                          "cores": threads, "kind": "reference", "sample": sample},
         "e2e": {"value": round(value, 2) if value else None, "unit": "GB/s",
@@ -751,7 +915,9 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--cpu-budget", type=float, default=20.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--ref-cases-per-step", type=int, default=4)
+    ap.add_argument("--ref-budget", type=float, default=150.0,
+                    help="seconds of reference CPU time after which no further timed step "
+                         "starts (--impl reference)")
     ap.add_argument("--tune-cache", default=DEFAULT_TUNE_CACHE,
                     help="autotune cache to load before planning (tiles tuned offline on "
                          "this GPU model by `python -m hptt_b200.tune_sweep`)")
@@ -766,6 +932,8 @@ def main():
     ap.add_argument("--serve-seconds", type=float, default=2.0,
                     help="arrival window per rate (60 for the full served workload)")
     ap.add_argument("--batch-reps", type=int, default=10)
+    ap.add_argument("--no-sections", action="store_true",
+                    help="skip the plain single transpose and hard-layout sections")
     ap.add_argument("--no-contraction", action="store_true",
                     help="skip the tensor-contraction (transpose-GEMM-transpose) section")
     ap.add_argument("--contract-reps", type=int, default=20)
