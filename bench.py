@@ -202,11 +202,15 @@ def _make_plans(cases, rank):
 
 
 def _timed_steps(plans, steps, warmup, stream, dist, world, flush=None):
-    """Warm-up, then `steps` timed steps (every transpose once per step) with
-    a CUDA event pair around every launch.  Returns the max-over-ranks device
-    time of the steps (ms), each plan's summed per-launch time (ms), and the
-    clock samples.  flush: an L2 flush run before every launch, outside the
-    per-launch events (the step time then counts per-launch times only)."""
+    """Warm-up, then two timed passes of `steps` steps (every transpose once
+    per step).  Pass 1 brackets the whole pass with one CUDA event pair: the
+    step time, launches back to back as a caller issues them (consecutive
+    launches overlap their launch and CTA start-up, see kernels.cu).  Pass 2
+    puts an event pair around every launch: each plan's summed per-launch
+    device time, for the roofline.  Returns the max-over-ranks time of pass 1
+    (ms), the per-plan times of pass 2 (ms) and the clock samples of both.
+    flush: an L2 flush before every launch, outside the per-launch events;
+    the step time is then the sum of the per-launch times."""
     import torch
     sptr = stream.cuda_stream
 
@@ -234,8 +238,11 @@ def _timed_steps(plans, steps, warmup, stream, dist, world, flush=None):
     torch.cuda.synchronize()
     t0.record(stream)
     for k in range(steps):
-        step(ev[k])
+        step()
     t1.record(stream)
+    torch.cuda.synchronize()
+    for k in range(steps):
+        step(ev[k])
     torch.cuda.synchronize()
     clocks = sampler.stop()
     per_launch_ms = [sum(ev[k][i][0].elapsed_time(ev[k][i][1]) for k in range(steps))

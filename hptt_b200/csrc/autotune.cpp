@@ -38,8 +38,9 @@ std::string gpu_name() {
 const char *env_path() { return std::getenv("HPTT_B200_TUNE_CACHE"); }
 
 // Cache file: one line per key,
-// "key|run vmin smem rows_min y_first iters full_side walk upd_exact"
-// (missing trailing fields read as 0, walk and upd_exact as 1).
+// "key|run vmin smem rows_min y_first iters full_side walk upd_exact nt
+//  grid_order"
+// (missing trailing fields read as 0, walk and upd_exact as 1, nt as 256).
 void read_cache_stream(std::istream &f) {
   std::string line;
   while (std::getline(f, line)) {
@@ -53,6 +54,8 @@ void read_cache_stream(std::istream &f) {
       if (!(v >> tp.full_side)) tp.full_side = 0;
       if (!(v >> tp.walk)) tp.walk = 1;
       if (!(v >> tp.upd_exact)) tp.upd_exact = 1;
+      if (!(v >> tp.nt) || (tp.nt != 256 && tp.nt != 512)) tp.nt = 256;
+      if (!(v >> tp.grid_order)) tp.grid_order = 0;
       g_cache[line.substr(0, bar)] = tp;
     }
   }
@@ -74,7 +77,8 @@ int write_cache(const char *path) {
     f << kv.first << "|" << kv.second.run_bytes << " " << kv.second.vmin_bytes << " "
       << kv.second.smem_bytes << " " << kv.second.rows_min_bytes << " "
       << kv.second.y_first << " " << kv.second.max_iters << " " << kv.second.full_side << " "
-      << kv.second.walk << " " << kv.second.upd_exact << "\n";
+      << kv.second.walk << " " << kv.second.upd_exact << " " << kv.second.nt << " "
+      << kv.second.grid_order << "\n";
   return ST_OK;
 }
 
@@ -98,6 +102,20 @@ std::vector<TileParams> candidates(int elem_size) {
             tp.full_side = full;
             c.push_back(tp);
           }
+  // 512-thread CTAs: twice the tile at the same per-thread iterations
+  // (longer runs on shapes whose contiguous extents are short)
+  for (int full : {0, 1, 2})
+    for (int yf : {0, 1})
+      for (int run : {256, 512})
+        for (int vmin : {16384, 32768}) {
+          TileParams tp;
+          tp.nt = 512;
+          tp.y_first = yf;
+          tp.run_bytes = run;
+          tp.vmin_bytes = vmin;
+          tp.full_side = full;
+          c.push_back(tp);
+        }
   return c;
 }
 
@@ -180,17 +198,20 @@ int autotune(Plan *p, double timeout, TileParams *best) {
     }
     return best;
   };
-  // After the grid of candidates, two alternative forms of the winner, each
-  // kept only if faster (which wins depends on the shape): its two-dim
-  // sides read from tables instead of walked, then, for update tiles, the
-  // general predicated path instead of exact trip counts.  A winner without
-  // such sides or tiles plans the same tile again, which the check below
-  // skips.
+  // After the grid of candidates, three alternative forms of the winner,
+  // each kept only if faster (which wins depends on the shape): the grid
+  // levels ordered by stride, its two-dim sides read from tables instead of
+  // walked, then, for update tiles, the general predicated path instead of
+  // exact trip counts.  A winner without such sides or tiles plans the same
+  // tile again, which the check below skips.
   int alt = 0;
-  for (size_t ci = 0; ci < cands.size() || (found && alt < 2); ++ci) {
+  for (size_t ci = 0; ci < cands.size() || (found && alt < 3); ++ci) {
     if (ci >= cands.size()) {
       TileParams tp = winner;
-      if (alt++ == 0)
+      const int which = alt++;
+      if (which == 0)
+        tp.grid_order = 1;
+      else if (which == 1)
         tp.walk = 0;
       else
         tp.upd_exact = 0;

@@ -20,7 +20,7 @@ using namespace dev;
 
 namespace {
 
-constexpr int kNT = 256;
+constexpr int kNT = kBatchThreads;
 // Tile bodies ("shapes"):
 //   0 tile, table offsets (uint32)      3 rows, widest vector (uint32)
 //   1 tile, single-dim sides (uint32)   4 rows, scalar (uint32)
@@ -238,6 +238,12 @@ int batch_layout(const std::vector<BatchEntry> &entries, int sms, BatchLayout *L
     } else {
       d.a.t = p->tile_scalar;
       d.a.tables = p->dtab_scalar;
+    }
+    if (d.a.t.nt != kNT) {
+      // a 512-thread plan: its tile planned for the batch kernels' 256
+      d.a.t = p->tile_batch;
+      d.a.tables = p->dtab_batch;
+      vec = 1;
     }
     int shape = shape_of(d.a.t, vec, d.a.p.dtype);
     if (shape < 0) {

@@ -88,6 +88,18 @@ int plan_tiles(Plan *p, const TileParams &params) {
   } else {
     p->dtab_scalar = p->dtab;
   }
+  if (p->args.t.nt != kBatchThreads) {
+    TileParams bp = params;
+    bp.nt = kBatchThreads;
+    bp.max_vec_bytes = elem_bytes(p->args.p.dtype);  // rows: the scalar form
+    st = choose_tile(p->args.p, bp, p->args.update, &p->tile_batch);
+    if (st != ST_OK) return st;
+    st = upload(p->args.p, p->tile_batch, &p->dtab_batch);
+    if (st != ST_OK) return st;
+  } else {
+    p->tile_batch = p->args.t;
+    p->dtab_batch = p->dtab;
+  }
   // grid: resident CTAs on every SM, capped by the tile count
   auto size_grid = [&](const HpttTile &t, int vec, int *grid) -> int {
     HpttArgs a = p->args;
@@ -142,9 +154,11 @@ int plan_enqueue(Plan *p, cudaStream_t stream) {
 
 void plan_free_tables(Plan *p) {
   if (p->dtab_scalar && p->dtab_scalar != p->dtab) cudaFree(p->dtab_scalar);
+  if (p->dtab_batch && p->dtab_batch != p->dtab) cudaFree(p->dtab_batch);
   if (p->dtab) cudaFree(p->dtab);
   p->dtab = nullptr;
   p->dtab_scalar = nullptr;
+  p->dtab_batch = nullptr;
 }
 
 }  // namespace hptt_b200

@@ -10,17 +10,32 @@ using namespace dev;
 
 namespace {
 
-constexpr int kNT = 256;
+// Threads per CTA: 256 or 512 (HpttTile::nt; the planner's TileParams.nt).
+constexpr int kMaxNT = 512;
 
 // One CTA per tile.  The arguments live in the parameter space
 // (__grid_constant__) and are read through a const reference.  Register
-// budgets: 8 resident CTAs per SM for 4-byte copy/scale tiles (32 registers;
-// measured +0.3 % over the sweep, up to +8 % on short-run shapes), 6 for
+// budgets, stated for 512-thread CTAs (twice as many of 256 threads): 2048
+// resident threads per SM for 4-byte copy/scale tiles (32 registers;
+// measured +0.3 % over the sweep, up to +8 % on short-run shapes), 1536 for
 // wider elements (the shared-memory limit at 32 KB a tile; at 32 registers
-// they spill), 4 when B is read too.
+// they spill), 1024 when B is read too.
+// Programmatic dependent launch: every launch may begin while the previous
+// kernel on its stream is still running.  Each CTA first waits until that
+// kernel has completed and its memory is visible (griddepcontrol.wait), so
+// no global access moves ahead of it; only the launch and the CTA prologue
+// overlap.  Each CTA then lets the next launch begin (it starts once every
+// CTA of this grid has reached this point, i.e. during the last wave).  Both
+// are no-ops when the launch was not made programmatic.
+__device__ __forceinline__ void pdl_enter() {
+  asm volatile("griddepcontrol.wait;\n" ::: "memory");
+  asm volatile("griddepcontrol.launch_dependents;\n" ::: "memory");
+}
+
 template <typename E, int MODE, bool UPD, typename OffT, bool LX, bool LY>
-__global__ void __launch_bounds__(kNT, UPD ? 4 : (sizeof(E) <= 4 ? 8 : 6))
+__global__ void __launch_bounds__(kMaxNT, UPD ? 2 : (sizeof(E) <= 4 ? 4 : 3))
     k_tile(const __grid_constant__ HpttArgs args) {
+  pdl_enter();
   extern __shared__ __align__(16) unsigned char smem[];
   const Scal sc{args.alpha[0], args.alpha[1], args.beta[0], args.beta[1]};
   const Op<E, MODE, UPD> op(sc);
@@ -31,7 +46,8 @@ __global__ void __launch_bounds__(kNT, UPD ? 4 : (sizeof(E) <= 4 ? 8 : 6))
 }
 
 template <typename E, int MODE, bool UPD, typename OffT, int VEC>
-__global__ void __launch_bounds__(kNT) k_rows(const __grid_constant__ HpttArgs args) {
+__global__ void __launch_bounds__(kMaxNT) k_rows(const __grid_constant__ HpttArgs args) {
+  pdl_enter();
   const Scal sc{args.alpha[0], args.alpha[1], args.beta[0], args.beta[1]};
   const Op<E, MODE, UPD> op(sc);
   rows_one<E, MODE, UPD, OffT, VEC>(args.p, args.t, static_cast<const E *>(args.A),
@@ -103,16 +119,25 @@ const void *kernel_for(const HpttArgs &a, int vec) {
   }
 }
 
-int kernel_threads() { return kNT; }
+int kernel_threads() { return kMaxNT; }
 
 cudaError_t launch_single(const HpttArgs &a, int vec, int grid, cudaStream_t stream) {
-  (void)grid;
+  (void)grid;  // one CTA per tile
   const void *fn = kernel_for(a, vec);
   if (!fn) return cudaErrorInvalidValue;
   if (a.t.num_tiles == 0) return cudaSuccess;
   void *params[] = {const_cast<HpttArgs *>(&a)};
-  return cudaLaunchKernel(fn, dim3(a.t.num_tiles), dim3(a.t.nt), params,
-                          static_cast<size_t>(a.t.smem_bytes), stream);
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(a.t.num_tiles);
+  cfg.blockDim = dim3(a.t.nt);
+  cfg.dynamicSmemBytes = static_cast<size_t>(a.t.smem_bytes);
+  cfg.stream = stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelExC(&cfg, fn, params);
 }
 
 cudaError_t occupancy(const HpttArgs &a, int vec, int *ctas_per_sm) {

@@ -11,7 +11,7 @@ namespace hptt_b200 {
 // KIND_ROWS (1 when the pointers are not aligned for the planned vector).
 const void *kernel_for(const HpttArgs &a, int vec);
 
-// Threads per CTA the kernels are compiled for.
+// Most threads per CTA the single-transpose kernels are compiled for.
 int kernel_threads();
 
 // Enqueue one transpose.  `grid` CTAs loop over the tiles.

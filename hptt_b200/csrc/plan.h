@@ -27,7 +27,14 @@ struct Plan {
   bool tuned = false;
   void *dtab = nullptr;         // device offset tables for args.t
   void *dtab_scalar = nullptr;  // ... and for tile_scalar (may alias dtab)
+  // the tile the batch kernels (256 threads per CTA) run: args.t / dtab
+  // when that has 256 threads, else the same parameters planned for 256
+  HpttTile tile_batch{};
+  void *dtab_batch = nullptr;
 };
+
+// Threads per CTA of the batch kernels.
+constexpr int kBatchThreads = 256;
 
 // Release the plan's device tables.
 void plan_free_tables(Plan *p);

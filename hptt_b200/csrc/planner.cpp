@@ -366,9 +366,11 @@ void fast_div_magic(uint32_t d, uint32_t *mul, int32_t *shr) {
 }
 
 void finish_grid(const HpttProblem &p, HpttTile *t, const int64_t *tile_ext,
-                 const std::vector<int> &chunk_first) {
+                 const std::vector<int> &chunk_first, int order = 0) {
   // grid dims: chunked tile dims first, then every dim not fully inside the
-  // tile in input order
+  // tile in input order (order 0) or by min(|stride in A|, |stride in B|)
+  // (order 1: the neighbours that continue a tile's runs in A or in B come
+  // next in tile order)
   t->ng = 0;
   bool used[HPTT_MAX_RANK] = {false};
   uint64_t tiles = 1;
@@ -384,8 +386,18 @@ void finish_grid(const HpttProblem &p, HpttTile *t, const int64_t *tile_ext,
   };
   for (int d : chunk_first)
     if (d >= 0 && !used[d]) add(d);
+  std::vector<int> rest;
   for (int d = 0; d < p.rank; ++d)
-    if (!used[d]) add(d);
+    if (!used[d]) rest.push_back(d);
+  if (order == 1) {
+    auto key = [&](int d) {
+      const int64_t a = p.sA[d] < 0 ? -p.sA[d] : p.sA[d];
+      const int64_t b = p.sB[d] < 0 ? -p.sB[d] : p.sB[d];
+      return std::min(a, b);
+    };
+    std::stable_sort(rest.begin(), rest.end(), [&](int x, int y) { return key(x) < key(y); });
+  }
+  for (int d : rest) add(d);
   t->num_tiles = tiles > 0x7fffffffULL ? 0 : static_cast<uint32_t>(tiles);
   for (int g = 0; g < t->ng; ++g) fast_div_magic(t->gcnt[g], &t->gmul[g], &t->gshr[g]);
 }
@@ -511,7 +523,7 @@ int choose_rows(const HpttProblem &p, const TileParams &tp, HpttTile *t) {
   t->J1 = static_cast<int32_t>(cdiv(TY, t->R1));
   t->WTY = t->W;
   t->LD = 0;
-  finish_grid(p, t, tile_ext, {t->wc, t->yc});
+  finish_grid(p, t, tile_ext, {t->wc, t->yc}, tp.grid_order);
   // in-tile offsets
   int64_t maxA = (t->W - 1) * p.sA[0], maxB = (t->W - 1) * p.sB[0];
   for (int i = 0; i < t->ny; ++i) {
@@ -783,7 +795,7 @@ int choose_tile(const HpttProblem &p, const TileParams &tp, int update, HpttTile
     if (c == 0) break;
   }
   t->LD = best_ld;
-  finish_grid(p, t, tile_ext, {t->xc, t->yc});
+  finish_grid(p, t, tile_ext, {t->xc, t->yc}, tp.grid_order);
 
   int64_t maxA = 0, maxB = 0;
   if (common) {

@@ -53,6 +53,10 @@ struct TileParams {
   int upd_exact = 1;       // update tiles with single-dim sides: exact trip
                            // counts in interior tiles (1) or the general
                            // predicated path (0); HpttTile::upd_exact
+  int grid_order = 0;      // grid levels after the chunked tile dims: in
+                           // input order (0), or by the smaller of each
+                           // dim's A and B strides (1), so tiles that share
+                           // partially written sectors run close in time
 };
 
 // Reference argument guard (src/hptt.cc:25-56) plus the one check the

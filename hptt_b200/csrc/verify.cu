@@ -394,8 +394,14 @@ extern "C" int hptt_cuda_debug_check_indexing(int dtype, uint32_t rank, const ui
   L.nB = s;
   // every planner knob the tuner tries: side order, both update settings,
   // both per-thread iteration limits, the whole-extent options, tables or
-  // walks for two-dim sides, exact or predicated update interiors
-  for (int variant = 0; variant < 24; ++variant) {
+  // walks for two-dim sides, exact or predicated update interiors, 256 or
+  // 512 threads per CTA, grid levels in input or stride order
+  for (int v = 0; v < 48; ++v) {
+    const int variant = v % 24;
+    tp.nt = v < 24 ? 256 : 512;
+    tp.grid_order = v < 24 ? 0 : 1;
+    // 512 threads: the default iteration limit only
+    if (v >= 24 && ((variant >> 2) & 1)) continue;
     const int update = variant & 1;
     tp.y_first = (variant >> 1) & 1;
     tp.max_iters = ((variant >> 2) & 1) ? hptt_jmax_tile(elem_bytes(P.dtype)) / 2 : 0;
@@ -409,7 +415,8 @@ extern "C" int hptt_cuda_debug_check_indexing(int dtype, uint32_t rank, const ui
     std::vector<unsigned char> tab;
     build_tables(P, T, &tab);
     // the single-transpose kernel, then (tiles) the batch kernels' forms
-    for (int model = 0; model < (T.kind == KIND_TILE ? 2 : 1); ++model) {
+    // (512-thread tiles are planned again for 256 threads in a batch)
+    for (int model = 0; model < (T.kind == KIND_TILE && T.nt == 256 ? 2 : 1); ++model) {
       std::vector<uint8_t> writes(static_cast<size_t>(L.nB), 0);
       uint64_t n = 0;
       int rc;

@@ -122,9 +122,9 @@ def test_valid_plan_without_device_raises():
 
 def test_tune_cache_round_trip(tmp_path):
     """Cache files: load merges entries (missing trailing fields -- the
-    iteration cap, the whole-extent option -- read as 0, the side walk and
-    the exact update form as 1), save writes every entry back, clear
-    empties."""
+    iteration cap, the whole-extent option, the grid order -- read as 0, the
+    side walk and the exact update form as 1, the threads per CTA as 256),
+    save writes every entry back, clear empties."""
     src = tmp_path / "in.cache"
     src.write_text(
         "NVIDIA B200 0 2 1,0 27 0|256 16384 32768 512 0\n"
@@ -138,9 +138,9 @@ def test_tune_cache_round_trip(tmp_path):
     out = tmp_path / "out.cache"
     h.tune_cache_save(str(out))
     lines = sorted(out.read_text().splitlines())
-    assert lines == ["NVIDIA B200 0 2 1,0 27 0|256 16384 32768 512 0 0 0 1 1",
-                     "NVIDIA B200 0 4 2,3,0,1 27 1|256 16384 32768 512 0 0 1 0 1",
-                     "NVIDIA B200 1 3 2,0,1 28 1|128 8192 32768 512 1 4 0 1 1"]
+    assert lines == ["NVIDIA B200 0 2 1,0 27 0|256 16384 32768 512 0 0 0 1 1 256 0",
+                     "NVIDIA B200 0 4 2,3,0,1 27 1|256 16384 32768 512 0 0 1 0 1 256 0",
+                     "NVIDIA B200 1 3 2,0,1 28 1|128 8192 32768 512 1 4 0 1 1 256 0"]
     h.tune_cache_clear()
     assert h.tune_cache_size() == 0
     with pytest.raises(h.HpttError):

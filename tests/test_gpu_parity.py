@@ -264,8 +264,8 @@ FORM_SHAPES = [
 @pytest.mark.parametrize("al,be", [(1.0, 0.0), (2.3, 4.2)])
 def test_tile_forms_match(tmp_path, name, size, perm, al, be):
     """The tuner's alternative tile forms, each forced through the tune cache
-    (tune once, rewrite the entry's walk / upd_exact fields, reload): every
-    form bit-exact against the oracle."""
+    (tune once, rewrite the entry's walk / upd_exact / threads / grid-order
+    fields, reload): every form bit-exact against the oracle."""
     rng = np.random.default_rng(17)
     n_in, n_out = footprint(size, perm)
     a = seeded(rng, n_in, name)
@@ -280,15 +280,16 @@ def test_tile_forms_match(tmp_path, name, size, perm, al, be):
         (line,) = path.read_text().splitlines()
         key, fields = line.split("|")
         f = fields.split()
-        assert len(f) == 9
-        for walk in (0, 1):
-            for exact in (0, 1):
-                f[7], f[8] = str(walk), str(exact)
-                path.write_text(key + "|" + " ".join(f) + "\n")
-                h.tune_cache_clear()
-                h.tune_cache_load(str(path))
-                got = gpu_run(name, size, perm, al, be, a, b0)
-                assert_same(got, want, name, f"{size} {perm} walk={walk} exact={exact}")
+        assert len(f) == 11
+        for walk, exact, nt, order in ((0, 0, 256, 0), (0, 1, 256, 0), (1, 0, 256, 0),
+                                       (1, 1, 256, 1), (1, 1, 512, 0), (0, 0, 512, 1)):
+            f[7], f[8], f[9], f[10] = str(walk), str(exact), str(nt), str(order)
+            path.write_text(key + "|" + " ".join(f) + "\n")
+            h.tune_cache_clear()
+            h.tune_cache_load(str(path))
+            got = gpu_run(name, size, perm, al, be, a, b0)
+            assert_same(got, want, name,
+                        f"{size} {perm} walk={walk} exact={exact} nt={nt} order={order}")
     finally:
         h.tune_cache_clear()
 
