@@ -88,9 +88,11 @@ int plan_tiles(Plan *p, const TileParams &params) {
   } else {
     p->dtab_scalar = p->dtab;
   }
-  if (p->args.t.nt != kBatchThreads) {
+  if (p->args.t.nt != kBatchThreads || p->args.t.kind == KIND_VTILE) {
+    // the batch kernels run the 256-thread tile and rows forms only
     TileParams bp = params;
     bp.nt = kBatchThreads;
+    bp.vt = 0;
     bp.max_vec_bytes = elem_bytes(p->args.p.dtype);  // rows: the scalar form
     st = choose_tile(p->args.p, bp, p->args.update, &p->tile_batch);
     if (st != ST_OK) return st;

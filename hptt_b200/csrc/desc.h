@@ -24,7 +24,10 @@ enum HpttMode : int32_t { MODE_COPY = 0, MODE_REAL = 1, MODE_CPLX = 2 };
 //              dims (Y) and go through shared memory.
 //   KIND_ROWS  the fused stride-1 dimension is shared by A and B: rows are
 //              copied/scaled directly, no shared-memory transpose.
-enum HpttKind : int32_t { KIND_TILE = 0, KIND_ROWS = 1 };
+//   KIND_VTILE tiles whose X side is one contiguous run of A and whose Y side
+//              is one contiguous run of B, moved as 16-byte vectors (see
+//              vtile.cuh); elements of at most 8 bytes.
+enum HpttKind : int32_t { KIND_TILE = 0, KIND_ROWS = 1, KIND_VTILE = 2 };
 
 // Fused problem.  Dimensions are listed in INPUT order; sA/sB are the strides
 // (in elements) of input dim d in A and in B.  perm[k] = input dim that is
@@ -108,6 +111,9 @@ struct HpttTile {
   //               X dims in OUTPUT order, so consecutive slots are adjacent in B
   //   [thr_off]   nt x HpttThr per-thread constants
   // KIND_ROWS: A row offsets (TY x OffT) at 0, B row offsets at tab2_off.
+  // KIND_VTILE: TY x OffT at 0, row y (Y dims in output order) -> A offset
+  // of the row; TX x OffT at tab2_off, column x (X dims in input order) ->
+  // B offset of the column.
   int32_t tab2_off, thr_off, table_bytes;
   // fast division by R1 and R2 (same scheme as gmul/gshr)
   uint32_t r1_mul, r2_mul;
@@ -129,6 +135,10 @@ struct HpttTile {
   // two-dim sides: the X side's column slots (B offsets, step R2) and the Y
   // side's row slots (A offsets, step R1)
   HpttWalk wx, wy;
+  // KIND_VTILE: log2 of the 8-slot groups along a row of the load phase
+  // (vlx) and along a column of the store phase (vly); a row has 8 << vlx
+  // vector slots, a column 8 << vly
+  int32_t vlx, vly;
 };
 
 // One slot of a KIND_TILE offset table (OffT = uint32_t or int64_t).

@@ -109,6 +109,7 @@ const void *pick_mode_cplx(int mode, bool upd, const HpttTile &t, int vec) {
 }  // namespace
 
 const void *kernel_for(const HpttArgs &a, int vec) {
+  if (a.t.kind == KIND_VTILE) return vtile_kernel_for(a);
   const bool upd = a.update != 0;
   switch (a.p.dtype) {
     case DT_F32: return pick_mode<float, unsigned int>(a.mode, upd, a.t, vec);

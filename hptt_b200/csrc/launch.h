@@ -11,6 +11,9 @@ namespace hptt_b200 {
 // KIND_ROWS (1 when the pointers are not aligned for the planned vector).
 const void *kernel_for(const HpttArgs &a, int vec);
 
+// The vector-tile kernel (KIND_VTILE) for these arguments, or null.
+const void *vtile_kernel_for(const HpttArgs &a);
+
 // Most threads per CTA the single-transpose kernels are compiled for.
 int kernel_threads();
 

@@ -10,6 +10,7 @@
 // upper one's stride equals the lower one's stride times its extent in both
 // A and B.  Extent-1 dims are dropped first (they never change an offset).
 #include "planner.h"
+#include "vtile.cuh"
 
 #include <algorithm>
 #include <cstdio>
@@ -540,7 +541,198 @@ int choose_rows(const HpttProblem &p, const TileParams &tp, HpttTile *t) {
   return t->num_tiles ? ST_OK : ST_TOO_LARGE;
 }
 
+// Shared-memory wavefronts beyond the ideal of a vector tile's accesses with
+// row pitch `ld`: the first row of every thread of the first warps in the
+// load phase (each of its window's V elements) and their first column in the
+// store phase, with the rows' and columns' window shifts taken from the
+// offsets (a tile origin on a 16-byte boundary).
+int vtile_bank_cost(const HpttTile &t, int ld, int sz, const std::vector<int64_t> &rowA,
+                    const std::vector<int64_t> &colB) {
+  const int V = 16 / sz, P = V - 1;
+  auto md = [V](int64_t v) { return static_cast<int>(((v % V) + V) % V); };
+  int cost = 0;
+  int64_t addr[32];
+  const int warps = std::min(t.nt / 32, 8);
+  for (int w = 0; w < warps; ++w) {
+    for (int i = 0; i < V; ++i) {
+      for (int l = 0; l < 32; ++l) {
+        const dev::VtPos ps = dev::vt_pos(w * 32 + l, t.vlx);
+        const int y = ps.r0;
+        addr[l] = -1;
+        if (y >= t.TY) continue;
+        const int sh = md(rowA[y]);
+        const int x = ps.k * V - sh + i;
+        if (ps.k * V - sh >= t.TX) continue;
+        addr[l] = (static_cast<int64_t>(y + P) * ld + x + P) * sz;
+      }
+      cost += excess_wavefronts(addr, 32, sz);
+      for (int l = 0; l < 32; ++l) {
+        const dev::VtPos ps = dev::vt_pos(w * 32 + l, t.vly);
+        const int x = ps.r0;
+        addr[l] = -1;
+        if (x >= t.TX) continue;
+        const int y0 = ps.k * V - md(colB[x]);
+        if (y0 >= t.TY) continue;
+        addr[l] = (static_cast<int64_t>(y0 + i + P) * ld + x + P) * sz;
+      }
+      cost += excess_wavefronts(addr, 32, sz);
+    }
+  }
+  return cost;
+}
+
+int log2_slots(int n) { return n >= 32 ? 2 : (n >= 16 ? 1 : 0); }
+
+// Vector tile (KIND_VTILE, vtile.cuh).  X: input dims 0, 1, ... whose A
+// strides chain (one contiguous run of A), never the output's leading dim;
+// Y: output dims 0, 1, ... not in X whose B strides chain (one run of B).
+// Each side takes whole dims while its run fits the window slots
+// (nvx * V - V + 1 elements: any start shift fits) and the per-thread
+// iterations, then a balanced chunk of the next dim.
+int choose_vtile(const HpttProblem &p, const TileParams &tp, HpttTile *t) {
+  const int sz = elem_bytes(p.dtype);
+  if (!vtile_possible(p)) return ST_TOO_LARGE;
+  const int V = 16 / sz, JV = dev::hptt_vt_jmax();
+  const int r = p.rank;
+  std::memset(t, 0, sizeof(*t));
+  t->kind = KIND_VTILE;
+  t->nt = tp.nt;
+  t->vec = V;
+  t->W = 1;
+  t->xc = t->yc = t->wc = -1;
+  auto fits = [](int n) { return n == 8 || n == 16 || n == 32; };
+  if (!fits(tp.vt_nvx) || !fits(tp.vt_nvy)) return ST_TOO_LARGE;
+  if (tp.nt / tp.vt_nvx < 4 || tp.nt / tp.vt_nvy < 4) return ST_TOO_LARGE;
+  bool in_x[HPTT_MAX_RANK] = {false};
+  int64_t tile_ext[HPTT_MAX_RANK];
+  for (int d = 0; d < r; ++d) tile_ext[d] = 1;
+  // X run: bounded by the load window and by the store phase's iterations
+  const int64_t txmax = std::min<int64_t>(tp.vt_nvx * V - V + 1, (tp.nt / tp.vt_nvy) * JV);
+  int64_t TX = 1;
+  for (int d = 0; d < r; ++d) {
+    if (d == p.perm[0]) break;
+    if (d == 0 ? p.sA[0] != 1 : p.sA[d] != p.sA[d - 1] * p.n[d - 1]) break;
+    if (TX * p.n[d] <= txmax) {
+      t->xd[t->nx] = d;
+      t->xt[t->nx++] = static_cast<int32_t>(p.n[d]);
+      TX *= p.n[d];
+      in_x[d] = true;
+      continue;
+    }
+    const int64_t c = txmax / TX;
+    if (c >= 2) {
+      const int64_t tt = cdiv(p.n[d], cdiv(p.n[d], c));
+      t->xd[t->nx] = d;
+      t->xt[t->nx++] = static_cast<int32_t>(tt);
+      TX *= tt;
+      in_x[d] = true;
+      t->xc = d;
+    }
+    break;
+  }
+  if (t->nx == 0) return ST_TOO_LARGE;
+  // fewest load slots that cover the run
+  int nvx = 8;
+  while (nvx * V - V + 1 < TX) nvx *= 2;
+  const int R1 = tp.nt / nvx;
+  const int64_t tymax = std::min<int64_t>(tp.vt_nvy * V - V + 1, static_cast<int64_t>(R1) * JV);
+  int64_t TY = 1;
+  for (int k = 0; k < r; ++k) {
+    const int d = p.perm[k];
+    if (in_x[d]) break;
+    if (k == 0 ? p.sB[d] != 1 : p.sB[d] != p.sB[p.perm[k - 1]] * p.n[p.perm[k - 1]]) break;
+    if (TY * p.n[d] <= tymax) {
+      t->yd[t->ny] = d;
+      t->yt[t->ny++] = static_cast<int32_t>(p.n[d]);
+      TY *= p.n[d];
+      continue;
+    }
+    const int64_t c = tymax / TY;
+    if (c >= 2) {
+      const int64_t tt = cdiv(p.n[d], cdiv(p.n[d], c));
+      t->yd[t->ny] = d;
+      t->yt[t->ny++] = static_cast<int32_t>(tt);
+      TY *= tt;
+      t->yc = d;
+    }
+    break;
+  }
+  if (t->ny == 0) return ST_TOO_LARGE;
+  int nvy = 8;
+  while (nvy * V - V + 1 < TY) nvy *= 2;
+  const int R2 = tp.nt / nvy;
+  if (cdiv(TY, R1) > JV || cdiv(TX, R2) > JV) return ST_TOO_LARGE;
+  t->vlx = log2_slots(nvx);
+  t->vly = log2_slots(nvy);
+  t->TX = static_cast<int32_t>(TX);
+  t->TY = static_cast<int32_t>(TY);
+  t->RW = t->TX;
+  t->WTY = t->TY;
+  t->R1 = R1;
+  t->J1 = static_cast<int32_t>(cdiv(TY, R1));
+  t->R2 = R2;
+  t->J2 = static_cast<int32_t>(cdiv(TX, R2));
+  t->px = 1;
+  t->py = 1;
+  for (int i = 0; i + 1 < t->nx; ++i) t->px *= t->xt[i];
+  for (int i = 0; i + 1 < t->ny; ++i) t->py *= t->yt[i];
+  for (int i = 0; i < t->nx; ++i) tile_ext[t->xd[i]] = t->xt[i];
+  for (int i = 0; i < t->ny; ++i) tile_ext[t->yd[i]] = t->yt[i];
+  finish_grid(p, t, tile_ext, {t->xc, t->yc}, tp.grid_order);
+  int64_t maxA = 0, maxB = 0;
+  for (int i = 0; i < t->nx; ++i) {
+    maxA += (t->xt[i] - 1) * p.sA[t->xd[i]];
+    maxB += (t->xt[i] - 1) * p.sB[t->xd[i]];
+  }
+  for (int i = 0; i < t->ny; ++i) {
+    maxA += (t->yt[i] - 1) * p.sA[t->yd[i]];
+    maxB += (t->yt[i] - 1) * p.sB[t->yd[i]];
+  }
+  t->big_offsets = (maxA + V >= 0x7fffffffLL || maxB + V >= 0x7fffffffLL);
+  const int off = t->big_offsets ? 8 : 4;
+  auto a16 = [](int64_t x) { return static_cast<int32_t>((x + 15) & ~int64_t(15)); };
+  t->tab2_off = a16(t->TY * off);
+  t->thr_off = t->tab2_off + a16(t->TX * off);
+  t->table_bytes = t->thr_off;
+  finish_tables(p, t);
+  // row pitch with the fewest bank conflicts (rows run from -(V-1), a row
+  // holds the window slots' span)
+  std::vector<int64_t> rowA, colB;
+  vtile_maps(p, *t, &rowA, &colB);
+  const int ld0 = nvx * V + V - 1;
+  int best_ld = ld0, best_cost = 1 << 30;
+  for (int ld = ld0; ld < ld0 + 128 / sz; ++ld) {
+    const int c = vtile_bank_cost(*t, ld, sz, rowA, colB);
+    if (c < best_cost) {
+      best_cost = c;
+      best_ld = ld;
+    }
+    if (c == 0) break;
+  }
+  t->LD = best_ld;
+  const int64_t rows = static_cast<int64_t>(nvy) * V + V - 1;
+  t->smem_bytes = a16(rows * t->LD * sz);
+  if (t->smem_bytes > tp.smem_bytes * 3) return ST_TOO_LARGE;
+  return t->num_tiles ? ST_OK : ST_TOO_LARGE;
+}
+
 }  // namespace
+
+bool vtile_possible(const HpttProblem &p) {
+  const int sz = elem_bytes(p.dtype);
+  return (sz == 4 || sz == 8) && p.rank >= 2 && p.perm[0] != 0;
+}
+
+void vtile_maps(const HpttProblem &p, const HpttTile &t, std::vector<int64_t> *rowA,
+                std::vector<int64_t> *colB) {
+  rowA->assign(static_cast<size_t>(t.TY), 0);
+  colB->assign(static_cast<size_t>(t.TX), 0);
+  int c = 0;
+  for (int y = 0; y < t.TY; ++y)
+    (*rowA)[y] = side_offset(y, t.ny, t.yd, t.yt, p.sA, -1, &c);
+  for (int x = 0; x < t.TX; ++x)
+    (*colB)[x] = side_offset(x, t.nx, t.xd, t.xt, p.sB, -1, &c);
+}
 
 int choose_tile(const HpttProblem &p, const TileParams &tp, int update, HpttTile *t) {
   (void)update;  // the shapes are the same with and without the B read
@@ -550,6 +742,7 @@ int choose_tile(const HpttProblem &p, const TileParams &tp, int update, HpttTile
   if (r == 1 || (common && p.n[0] * sz >= tp.rows_min_bytes))
     return choose_rows(p, tp, t);
   if (common && p.n[0] > tp.nt / 2) return choose_rows(p, tp, t);
+  if (tp.vt && vtile_possible(p) && choose_vtile(p, tp, t) == ST_OK) return ST_OK;
 
   std::memset(t, 0, sizeof(*t));
   t->kind = KIND_TILE;
@@ -839,9 +1032,14 @@ std::string describe(const HpttProblem &p, const HpttTile &t) {
   for (int d = 0; d < p.rank; ++d) os << " " << p.sA[d];
   os << "\n  strides B:";
   for (int d = 0; d < p.rank; ++d) os << " " << p.sB[d];
-  os << "\nkernel: " << (t.kind == KIND_TILE ? "tile (shared-memory transpose)" : "rows (shared stride-1)")
+  os << "\nkernel: "
+     << (t.kind == KIND_TILE    ? "tile (shared-memory transpose)"
+         : t.kind == KIND_VTILE ? "vector tile (16-byte windows, shared-memory transpose)"
+                                : "rows (shared stride-1)")
      << ", " << t.nt << " threads/CTA";
   if (t.kind == KIND_ROWS) os << ", vector " << t.vec;
+  if (t.kind == KIND_VTILE)
+    os << ", slots " << (8 << t.vlx) << " x " << (8 << t.vly) << ", J " << t.J1 << "/" << t.J2;
   os << "\n  tile W=" << t.W << " X{";
   for (int i = 0; i < t.nx; ++i) os << (i ? "," : "") << t.xd[i] << ":" << t.xt[i];
   os << "} Y{";

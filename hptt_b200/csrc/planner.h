@@ -57,7 +57,15 @@ struct TileParams {
                            // input order (0), or by the smaller of each
                            // dim's A and B strides (1), so tiles that share
                            // partially written sectors run close in time
+  int vt = 0;              // 1: a vector tile (KIND_VTILE) where the shape
+                           // allows one, else the tile above
+  int vt_nvx = 16;         // vector slots along a row (load) and along a
+  int vt_nvy = 16;         // column (store) of a vector tile: 8, 16 or 32
 };
+
+// Whether a vector tile (KIND_VTILE) can serve this problem: elements of at
+// most 8 bytes and no shared stride-1 dim.
+bool vtile_possible(const HpttProblem &p);
 
 // Reference argument guard (src/hptt.cc:25-56) plus the one check the
 // reference omits for memory safety (out_outer[k] >= out_size[k]).
@@ -88,6 +96,12 @@ struct TileMaps {
   std::vector<int> cx;        // column slot -> coordinate along the chunked X dim
 };
 void tile_maps(const HpttProblem &p, const HpttTile &t, TileMaps *m);
+
+// Host-side index maps of a KIND_VTILE tile: rowA[y] = A offset of row y
+// (the Y dims in output order), colB[x] = B offset of column x (the X dims in
+// input order).
+void vtile_maps(const HpttProblem &p, const HpttTile &t, std::vector<int64_t> *rowA,
+                std::vector<int64_t> *colB);
 
 // Per-thread constants of thread `tid` (uses t.LD).
 HpttThr tile_thread_consts(const HpttProblem &p, const HpttTile &t, const TileMaps &m, int tid);

@@ -28,6 +28,13 @@ void build_typed(const HpttProblem &P, const HpttTile &T, unsigned char *base) {
     }
     HpttThr *thr = reinterpret_cast<HpttThr *>(base + T.thr_off);
     for (int t = 0; t < T.nt; ++t) thr[t] = tile_thread_consts(P, T, m, t);
+  } else if (T.kind == KIND_VTILE) {
+    std::vector<int64_t> rowA, colB;
+    vtile_maps(P, T, &rowA, &colB);
+    OffT *ra = reinterpret_cast<OffT *>(base);
+    OffT *cb = reinterpret_cast<OffT *>(base + T.tab2_off);
+    for (int y = 0; y < T.TY; ++y) ra[y] = static_cast<OffT>(rowA[y]);
+    for (int x = 0; x < T.TX; ++x) cb[x] = static_cast<OffT>(colB[x]);
   } else {
     dev::rows_tables<OffT>(P, T, reinterpret_cast<OffT *>(base),
                            reinterpret_cast<OffT *>(base + T.tab2_off), 0, 1);

@@ -17,6 +17,7 @@
 #include "kernels.cuh"
 #include "planner.h"
 #include "tables.h"
+#include "vtile.cuh"
 
 namespace hptt_b200 {
 namespace {
@@ -311,6 +312,120 @@ int replay_tile(const HpttProblem &P, const HpttTile &T, int update, const Layou
   return 0;
 }
 
+// Vector tile (vtile.cuh: vtile_one), with the A and B base addresses
+// `misA` / `misB` elements past a 16-byte boundary.  Every window the kernel
+// reads must be 16-byte aligned and hold at least one element of its buffer
+// (so it lies in the buffer's own 16-byte blocks); every 16-byte store must be
+// aligned and wholly inside the column; every shared-memory access must stay
+// inside the tile buffer, and the store phase must read, for each element it
+// writes, the slot the load phase filled with the A element the permutation
+// maps to it.
+template <typename OffT>
+int replay_vtile(const HpttProblem &P, const HpttTile &T, int update, const Layout &L,
+                 const std::vector<unsigned char> &tab, std::vector<uint8_t> &writes,
+                 uint64_t *checked, int misA, int misB) {
+  const int esz = elem_bytes(P.dtype);
+  const int V = 16 / esz, PD = V - 1;
+  const int JV = hptt_vt_jmax();
+  if (V < 2) return 301;
+  if (T.J1 > JV || T.J2 > JV) return 302;
+  const int nvx = 8 << T.vlx, nvy = 8 << T.vly;
+  if (T.R1 != T.nt / nvx || T.R2 != T.nt / nvy) return 303;
+  if (T.R1 * T.J1 < T.TY || T.R2 * T.J2 < T.TX) return 304;
+  if (nvx * V - PD < T.TX || nvy * V - PD < T.TY) return 305;
+  if (T.LD < nvx * V + PD) return 306;
+  const int64_t rows = static_cast<int64_t>(nvy) * V + PD;
+  if (T.smem_bytes < rows * T.LD * esz) return 307;
+  if (T.tab2_off < T.TY * static_cast<int>(sizeof(OffT))) return 308;
+  if (T.table_bytes < T.tab2_off + T.TX * static_cast<int>(sizeof(OffT))) return 309;
+  const OffT *tabY = reinterpret_cast<const OffT *>(tab.data());
+  const OffT *tabX = reinterpret_cast<const OffT *>(tab.data() + T.tab2_off);
+  const bool ly = !T.big_offsets && T.ny <= 1, lx = !T.big_offsets && T.nx <= 1;
+  // the kernel computes single-dim sides as q * stride in 32 bits: the
+  // tables must hold exactly that
+  for (int y = 0; y < T.TY; ++y) {
+    const int64_t want = ly && T.ny == 1 ? static_cast<int64_t>(y) * T.sya : static_cast<int64_t>(tabY[y]);
+    if (static_cast<int64_t>(tabY[y]) != want) return 310;
+    if (ly && want > 0x7fffffffLL) return 311;
+  }
+  for (int x = 0; x < T.TX; ++x) {
+    const int64_t want = lx && T.nx == 1 ? static_cast<int64_t>(x) * T.sxb : static_cast<int64_t>(tabX[x]);
+    if (static_cast<int64_t>(tabX[x]) != want) return 312;
+    if (lx && want > 0x7fffffffLL) return 313;
+  }
+  auto md = [V](int64_t v) { return static_cast<int>(((v % V) + V) % V); };
+  const int64_t smem_elems = rows * T.LD;
+  std::vector<int64_t> slot(static_cast<size_t>(smem_elems));
+  // does [w, w + V) (elements from the buffer base) hold an element of [0, n)?
+  auto window_ok = [V](int64_t w, int64_t n) { return w + V > 0 && w < n; };
+  for (uint32_t tile = 0; tile < T.num_tiles; ++tile) {
+    const TileOrigin o = tile_origin(P, T, tile);
+    const int limX = vt_lim_x(T, o), limY = vt_lim_y(T, o);
+    if (limX < 1 || limY < 1 || limX > T.TX || limY > T.TY) return 314;
+    std::fill(slot.begin(), slot.end(), -1);
+    for (int t = 0; t < T.nt; ++t) {
+      const VtPos ps = vt_pos(t, T.vlx);
+      if (ps.k >= nvx || ps.r0 >= T.R1) return 315;
+      const int xk = ps.k * V;
+      for (int j = 0; j < JV; ++j) {
+        const int y = ps.r0 + j * T.R1;
+        if (!(j < T.J1 && y < limY)) continue;
+        const int64_t row = o.bA + static_cast<int64_t>(tabY[y]);  // element index in A
+        const int sh = md(misA + row);
+        if (!(xk - sh < limX)) continue;
+        const int64_t w = row - sh + xk;
+        if (md(misA + w) != 0) return 316;        // 16-byte aligned window
+        if (!window_ok(w, L.nA)) return 317;     // inside the buffer's blocks
+        for (int i = 0; i < V; ++i) {
+          const int x = xk - sh + i;
+          const int64_t si = static_cast<int64_t>(y + PD) * T.LD + x + PD;
+          if (si < 0 || si >= smem_elems) return 318;
+          if (x < 0 || x >= limX) continue;      // padding, never read
+          if (slot[si] >= 0) return 319;         // two writers of one slot
+          const int64_t ia = w + i;
+          if (ia < 0 || ia >= L.nA) return 320;
+          if (ia != row + x) return 321;
+          slot[si] = ia;
+        }
+      }
+    }
+    for (int t = 0; t < T.nt; ++t) {
+      const VtPos ps = vt_pos(t, T.vly);
+      if (ps.k >= nvy || ps.r0 >= T.R2) return 322;
+      const int yk = ps.k * V;
+      for (int j = 0; j < JV; ++j) {
+        const int x = ps.r0 + j * T.R2;
+        if (!(j < T.J2 && x < limX)) continue;
+        const int64_t col = o.bB + static_cast<int64_t>(tabX[x]);  // element index in B
+        const int tt = md(misB + col);
+        const int y0 = yk - tt;
+        if (!(y0 < limY)) continue;
+        const int64_t w = col - tt + yk;
+        if (md(misB + w) != 0) return 323;
+        if (update && !window_ok(w, L.nB)) return 324;  // the B window read
+        const bool full = y0 >= 0 && y0 + V <= limY;
+        for (int i = 0; i < V; ++i) {
+          const int y = y0 + i;
+          const int64_t si = static_cast<int64_t>(y + PD) * T.LD + x + PD;
+          if (si < 0 || si >= smem_elems) return 325;
+          if (y < 0 || y >= limY) continue;      // not stored
+          const int64_t ia = slot[si];
+          if (ia < 0) return 326;                // reads a slot no load wrote
+          const int64_t ib = w + i;
+          if (ib < 0 || ib >= L.nB) return 327;
+          if (ib != col + y) return 328;
+          if (map_a_to_b(L, ia) != ib) return 329;
+          if (writes[ib] != 0) return 330;
+          writes[ib] = 1;
+          ++*checked;
+        }
+        (void)full;
+      }
+    }
+  }
+  return 0;
+}
+
 template <typename OffT>
 int replay_rows(const HpttProblem &P, const HpttTile &T, const Layout &L,
                 const std::vector<unsigned char> &tab, std::vector<uint8_t> &writes,
@@ -363,20 +478,20 @@ int replay_rows(const HpttProblem &P, const HpttTile &T, const Layout &L,
 
 using namespace hptt_b200;
 
-extern "C" int hptt_cuda_debug_check_indexing(int dtype, uint32_t rank, const uint32_t *in_size,
-                                              const uint32_t *perm, const uint32_t *in_outer,
-                                              const uint32_t *out_outer, int max_vec_bytes,
-                                              uint64_t *checked) {
+namespace hptt_b200 {
+namespace {
+
+// Guard, fusion and the host-side layout of a replayed problem.
+int replay_setup(int dtype, uint32_t rank, const uint32_t *in_size, const uint32_t *perm,
+                 const uint32_t *in_outer, const uint32_t *out_outer, HpttProblem *P,
+                 Layout *Lp, std::vector<uint8_t> *inner) {
   if (elem_bytes(dtype) == 0) return HPTT_ERR_DTYPE;
   int st = validate(static_cast<int>(rank), in_size, perm, in_outer, out_outer,
                     in_outer ? static_cast<int>(rank) : 0, out_outer ? static_cast<int>(rank) : 0);
   if (st != ST_OK) return st;
-  HpttProblem P;
-  st = fuse(dtype, static_cast<int>(rank), in_size, perm, in_outer, out_outer, &P);
+  st = fuse(dtype, static_cast<int>(rank), in_size, perm, in_outer, out_outer, P);
   if (st != ST_OK) return st;
-  TileParams tp;
-  if (max_vec_bytes > 0) tp.max_vec_bytes = max_vec_bytes;
-  Layout L;
+  Layout &L = *Lp;
   L.rank = static_cast<int>(rank);
   for (uint32_t d = 0; d < rank; ++d) {
     L.in_size.push_back(in_size[d]);
@@ -392,6 +507,43 @@ extern "C" int hptt_cuda_debug_check_indexing(int dtype, uint32_t rank, const ui
     s *= L.out_outer[k];
   }
   L.nB = s;
+  // which B elements are inside the tensor (not outer-size padding)
+  inner->assign(static_cast<size_t>(L.nB), 0);
+  for (int64_t ib = 0; ib < L.nB; ++ib) (*inner)[ib] = b_is_inner(L, ib) ? 1 : 0;
+  return ST_OK;
+}
+
+// Replays one vector tile with the given base misalignments; 0 or a code.
+int replay_vtile_form(const HpttProblem &P, const Layout &L, const std::vector<uint8_t> &inner,
+                      const HpttTile &T, int update, int misA, int misB, uint64_t *checked) {
+  std::vector<unsigned char> tab;
+  build_tables(P, T, &tab);
+  std::vector<uint8_t> writes(static_cast<size_t>(L.nB), 0);
+  uint64_t n = 0;
+  const int rc = T.big_offsets
+                     ? replay_vtile<int64_t>(P, T, update, L, tab, writes, &n, misA, misB)
+                     : replay_vtile<uint32_t>(P, T, update, L, tab, writes, &n, misA, misB);
+  if (rc != 0) return 2000 + rc;
+  for (int64_t ib = 0; ib < L.nB; ++ib)
+    if (writes[ib] != inner[ib]) return 2300;
+  if (checked) *checked = n;
+  return 0;
+}
+
+}  // namespace
+}  // namespace hptt_b200
+
+extern "C" int hptt_cuda_debug_check_indexing(int dtype, uint32_t rank, const uint32_t *in_size,
+                                              const uint32_t *perm, const uint32_t *in_outer,
+                                              const uint32_t *out_outer, int max_vec_bytes,
+                                              uint64_t *checked) {
+  HpttProblem P;
+  Layout L;
+  std::vector<uint8_t> inner;
+  int st = replay_setup(dtype, rank, in_size, perm, in_outer, out_outer, &P, &L, &inner);
+  if (st != ST_OK) return st;
+  TileParams tp;
+  if (max_vec_bytes > 0) tp.max_vec_bytes = max_vec_bytes;
   // every planner knob the tuner tries: side order, both update settings,
   // both per-thread iteration limits, the whole-extent options, tables or
   // walks for two-dim sides, exact or predicated update interiors, 256 or
@@ -429,9 +581,65 @@ extern "C" int hptt_cuda_debug_check_indexing(int dtype, uint32_t rank, const ui
                            : replay_rows<uint32_t>(P, T, L, tab, writes, &n);
       if (rc != 0) return 1000 + rc + (model ? 500 : 0);
       for (int64_t ib = 0; ib < L.nB; ++ib)
-        if (static_cast<bool>(writes[ib]) != b_is_inner(L, ib)) return 1300;
+        if (writes[ib] != inner[ib]) return 1300;
       if (checked) *checked = n;
     }
   }
+  // vector tiles: window-slot shapes and thread counts the tuner tries, both
+  // grid orders, and A/B base addresses on and off a 16-byte boundary.  The
+  // vector tile's shape does not depend on whether B is read, so one replay
+  // with the B-window checks covers both settings.
+  if (vtile_possible(P)) {
+    const int V = 16 / elem_bytes(P.dtype);
+    const int shapes[][4] = {{256, 16, 16, 0}, {256, 16, 32, 1}, {512, 32, 32, 0},
+                             {256, 32, 8, 1},  {512, 8, 32, 0}};
+    for (const auto &sh : shapes) {
+      {
+        const int update = 1;
+        TileParams vp;
+        vp.vt = 1;
+        vp.nt = sh[0];
+        vp.vt_nvx = sh[1];
+        vp.vt_nvy = sh[2];
+        vp.grid_order = sh[3];
+        HpttTile T;
+        st = choose_tile(P, vp, update, &T);
+        if (st != ST_OK) return st;
+        if (T.kind != KIND_VTILE) continue;  // the tile form, replayed above
+        for (int m = 0; m < 4; ++m) {
+          const int misA = (m & 1) ? V - 1 : 0;
+          const int misB = (m == 1 || m == 2) ? V - 1 : (m == 3 ? 1 : 0);
+          uint64_t n = 0;
+          const int rc = replay_vtile_form(P, L, inner, T, update, misA, misB, &n);
+          if (rc != 0) return rc;
+          if (checked && *checked != n) return 2301;
+        }
+      }
+    }
+  }
   return 0;
+}
+
+extern "C" int hptt_cuda_debug_check_vtile(int dtype, uint32_t rank, const uint32_t *in_size,
+                                           const uint32_t *perm, const uint32_t *in_outer,
+                                           const uint32_t *out_outer, int nt, int nvx, int nvy,
+                                           int grid_order, int update, int mis_a, int mis_b,
+                                           uint64_t *checked) {
+  HpttProblem P;
+  Layout L;
+  std::vector<uint8_t> inner;
+  if (checked) *checked = 0;
+  int st = replay_setup(dtype, rank, in_size, perm, in_outer, out_outer, &P, &L, &inner);
+  if (st != ST_OK) return st;
+  TileParams vp;
+  vp.vt = 1;
+  vp.nt = nt;
+  vp.vt_nvx = nvx;
+  vp.vt_nvy = nvy;
+  vp.grid_order = grid_order;
+  HpttTile T;
+  st = choose_tile(P, vp, update, &T);
+  if (st != ST_OK) return st;
+  if (T.kind != KIND_VTILE) return 0;
+  return replay_vtile_form(P, L, inner, T, update, mis_a, mis_b, checked);
 }

@@ -122,3 +122,53 @@ def test_replay_random_ranks_7_and_8(seed):
     rc, n = check(dt, size, perm)
     assert rc == 0, (dt, size, perm, rc)
     assert n == np.prod(size)
+
+
+def check_vtile(dtype, size, perm, nt, nvx, nvy, order, update, mis_a, mis_b):
+    lib = h.load_library()
+    f = lib.hptt_cuda_debug_check_vtile
+    f.argtypes = [ctypes.c_int, ctypes.c_uint32, _u32p, _u32p, _u32p, _u32p] + \
+        [ctypes.c_int] * 7 + [ctypes.POINTER(ctypes.c_uint64)]
+    f.restype = ctypes.c_int
+    u = lambda v: (ctypes.c_uint32 * len(v))(*v)  # noqa: E731
+    n = ctypes.c_uint64(0)
+    rc = f(h.dtype_code(dtype), len(size), u(size), u(perm), None, None, nt, nvx, nvy, order,
+           update, mis_a, mis_b, ctypes.byref(n))
+    return rc, n.value
+
+
+# The vector-tile shapes of the GPU tests, and small shapes with the sweep
+# workload's structure (odd extents, multi-dim runs, tiny runs).
+VTILE_SHAPES = [
+    ("f32", [500, 333], [1, 0]),
+    ("f32", [37, 29, 23], [2, 1, 0]),
+    ("f64", [233, 66, 17], [1, 0, 2]),
+    ("c64", [70, 41], [1, 0]),
+    ("f32", [30, 4, 34, 6, 5, 3], [2, 5, 1, 4, 0, 3]),
+    ("f32", [4, 6, 101, 57, 4], [4, 2, 3, 0, 1]),
+    ("f64", [17, 20, 46, 3, 2, 4], [4, 2, 3, 5, 1, 0]),
+    ("c64", [5, 3, 7, 40, 9], [3, 4, 0, 2, 1]),
+    ("f32", [67, 45, 9], [2, 0, 1]),
+    ("f32", [983, 16, 5, 3], [3, 0, 1, 2]),
+    ("f32", [12, 4, 4, 11, 19, 13], [4, 0, 5, 3, 1, 2]),
+    ("f64", [4, 18, 94, 7, 5], [4, 2, 0, 3, 1]),
+]
+
+
+@pytest.mark.parametrize("dt,size,perm", VTILE_SHAPES)
+def test_replay_vtile_every_tuner_form(dt, size, perm):
+    """Every window-slot shape, thread count and grid order the autotuner
+    times, with both update settings and base addresses on and off a 16-byte
+    boundary."""
+    v = 16 // {"f32": 4, "f64": 8, "c64": 8}[dt]
+    used = 0
+    for nt in (256, 512):
+        for nvx in (8, 16, 32):
+            for nvy in (8, 16, 32):
+                for order in (0, 1):
+                    for update, ma, mb in ((0, 0, 0), (1, v - 1, 1)):
+                        rc, n = check_vtile(dt, size, perm, nt, nvx, nvy, order, update, ma, mb)
+                        assert rc == 0, (dt, size, perm, nt, nvx, nvy, order, update, ma, mb, rc)
+                        assert n in (0, np.prod(size))
+                        used += n > 0
+    assert used > 0, "no vector tile planned"
