@@ -195,27 +195,34 @@ def _make_plans(cases, rank):
         p = h.create_plan(a, b, c["in_size"], c["perm"], c["alpha"], c["beta"], 0,
                           dtype=c["dtype"])
         assert p is not None
-        kind = "rows" if "kernel: rows" in p.describe() else "tile"
+        d = p.describe()
+        kind = ("rows" if "kernel: rows" in d else
+                "vtile" if "kernel: vector tile" in d else "tile")
         plans.append((p, algorithmic_bytes(c), kind, c))
     torch.cuda.synchronize()
     return plans, bufs
 
 
 def _timed_steps(plans, steps, warmup, stream, dist, world, flush=None):
-    """Warm-up, then two timed passes of `steps` steps (every transpose once
-    per step).  Pass 1 brackets the whole pass with one CUDA event pair: the
-    step time, launches back to back as a caller issues them (consecutive
-    launches overlap their launch and CTA start-up, see kernels.cu).  Pass 2
-    puts an event pair around every launch: each plan's summed per-launch
-    device time, for the roofline.  Returns the max-over-ranks time of pass 1
-    (ms), the per-plan times of pass 2 (ms) and the clock samples of both.
-    flush: an L2 flush before every launch, outside the per-launch events;
-    the step time is then the sum of the per-launch times."""
+    """Warm-up, then the timed passes.  Pass 1 brackets `steps` steps (every
+    transpose once per step, launched back to back as a caller issues them;
+    consecutive launches overlap their launch and CTA start-up, see
+    kernels.cu) with one CUDA event pair: the step time.  Pass 2, for the
+    roofline, runs `steps` steps of each kernel kind alone -- that kind's
+    transposes, in workload order, back to back -- between one event pair
+    per kind: each kernel's average launch duration in a stream of its own
+    launches.  Returns the max-over-ranks time of pass 1 (ms), the per-kind
+    times of pass 2 (ms, summed over the steps) and the clock samples.
+    flush: an L2 flush before every launch, outside per-launch event pairs;
+    the step time and the kind times are then sums of per-launch times."""
     import torch
     sptr = stream.cuda_stream
+    kinds = sorted({k for _, _, k, _ in plans})
 
-    def step(record=None):
-        for i, (p, _, _, _) in enumerate(plans):
+    def step(record=None, only=None):
+        for i, (p, _, kind, _) in enumerate(plans):
+            if only is not None and kind != only:
+                continue
             if flush is not None:
                 flush()
             if record is not None:
@@ -224,6 +231,9 @@ def _timed_steps(plans, steps, warmup, stream, dist, world, flush=None):
             if record is not None:
                 record[i][1].record(stream)
 
+    def ev():
+        return torch.cuda.Event(enable_timing=True)
+
     for _ in range(warmup):
         step()
     torch.cuda.synchronize()
@@ -231,52 +241,75 @@ def _timed_steps(plans, steps, warmup, stream, dist, world, flush=None):
         dist.barrier()
     sampler = ClockSampler(int(os.environ.get("LOCAL_RANK", "0")))
     sampler.start()
-    ev = [[(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
-           for _ in plans] for _ in range(steps)]
-    t0 = torch.cuda.Event(enable_timing=True)
-    t1 = torch.cuda.Event(enable_timing=True)
-    torch.cuda.synchronize()
-    t0.record(stream)
-    for k in range(steps):
-        step()
-    t1.record(stream)
-    torch.cuda.synchronize()
-    for k in range(steps):
-        step(ev[k])
-    torch.cuda.synchronize()
+    kind_ms = {}
+    if flush is None:
+        t0, t1 = ev(), ev()
+        torch.cuda.synchronize()
+        t0.record(stream)
+        for k in range(steps):
+            step()
+        t1.record(stream)
+        torch.cuda.synchronize()
+        elapsed_ms = t0.elapsed_time(t1)
+        for kind in kinds:
+            k0, k1 = ev(), ev()
+            k0.record(stream)
+            for k in range(steps):
+                step(only=kind)
+            k1.record(stream)
+            torch.cuda.synchronize()
+            kind_ms[kind] = k0.elapsed_time(k1)
+    else:
+        rec = [[(ev(), ev()) for _ in plans] for _ in range(steps)]
+        for k in range(steps):
+            step(rec[k])
+        torch.cuda.synchronize()
+        per_launch = [sum(rec[k][i][0].elapsed_time(rec[k][i][1]) for k in range(steps))
+                      for i in range(len(plans))]
+        for (_, _, kind, _), ms in zip(plans, per_launch):
+            kind_ms[kind] = kind_ms.get(kind, 0.0) + ms
+        elapsed_ms = sum(per_launch)
     clocks = sampler.stop()
-    per_launch_ms = [sum(ev[k][i][0].elapsed_time(ev[k][i][1]) for k in range(steps))
-                     for i in range(len(plans))]
-    elapsed_ms = sum(per_launch_ms) if flush is not None else t0.elapsed_time(t1)
     elapsed_ms = max_over_ranks(elapsed_ms, dist, world)
-    return elapsed_ms, per_launch_ms, clocks
+    return elapsed_ms, kind_ms, clocks
 
 
-def _roofline(plans, per_launch_ms, steps, traffic_ratio=None):
-    """The dominant kernel kind (most device time): its algorithmic bytes per
-    launch over its average launch duration, against the measured peak."""
+KERNEL_OF_KIND = {"tile": "k_tile", "vtile": "k_vtile", "rows": "k_rows"}
+
+
+def _roofline(plans, kind_ms, steps, traffic=None):
+    """The dominant kernel (most device time): its algorithmic bytes per
+    launch over its average launch duration (kind_ms from _timed_steps),
+    against the measured peak.  traffic: DRAM bytes per algorithmic byte of
+    that kernel from the committed single-launch captures, or None."""
     by_kind = {}
-    for (p, bb, kind, _), ms in zip(plans, per_launch_ms):
-        d = by_kind.setdefault(kind, [0.0, 0, 0])
-        d[0] += ms
-        d[1] += bb * steps
-        d[2] += steps
-    device_ms = sum(per_launch_ms)
-    dom = max(by_kind, key=lambda k: by_kind[k][0])
-    dom_ms, dom_bytes, dom_launches = by_kind[dom]
+    for p, bb, kind, _ in plans:
+        d = by_kind.setdefault(kind, [0, 0])
+        d[0] += bb * steps
+        d[1] += steps
+    device_ms = sum(kind_ms.values())
+    dom = max(kind_ms, key=lambda k: kind_ms[k])
+    dom_ms = kind_ms[dom]
+    dom_bytes, dom_launches = by_kind[dom]
     peak, peak_kind = _peaks()
     achieved = dom_bytes / (dom_ms / 1e3) / 1e9
     per_launch = int(dom_bytes // max(1, dom_launches))
+    ratio = (traffic or {}).get(KERNEL_OF_KIND[dom])
     return {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak,
             "unit": "GB/s", "frac": round(achieved / peak, 4),
-            "traffic": int(per_launch * traffic_ratio) if traffic_ratio else None,
-            "kernel": "k_tile" if dom == "tile" else "k_rows",
+            "traffic": int(per_launch * ratio) if ratio else None,
+            "kernel": KERNEL_OF_KIND[dom],
             "peak_source": ("measured (MEASURED_PEAKS.json hbm_gbs, burst copy)"
                             if peak_kind == "measured" else
                             "fallback 6650 GB/s (MEASURED_PEAKS.json absent)"),
             "launches": dom_launches,
             "algorithmic_bytes_per_launch": per_launch,
-            "share_of_device_time": round(dom_ms / device_ms, 4)}
+            "share_of_device_time": round(dom_ms / device_ms, 4),
+            "timing": "that kernel's transposes alone, back to back, one event pair per pass",
+            "kernels": {KERNEL_OF_KIND[k]: {"ms_per_step": round(kind_ms[k] / steps, 4),
+                                            "GB/s": round(by_kind[k][0] / (kind_ms[k] / 1e3) / 1e9, 1),
+                                            "launches_per_step": by_kind[k][1] // steps}
+                        for k in kind_ms}}
 
 
 def _l2_flush():
@@ -297,7 +330,7 @@ def run_section(args, name, stream):
     plans, bufs = _make_plans(cases, 0)
     flush = _l2_flush() if name == "plain" else None
     steps = 50 if name == "plain" else 20
-    ms, per_launch, clocks = _timed_steps(plans, steps, 3, stream, None, 1, flush=flush)
+    ms, kind_ms, clocks = _timed_steps(plans, steps, 3, stream, None, 1, flush=flush)
     bytes_step = sum(bb for _, bb, _, _ in plans)
     peak, _ = _peaks()
     value = bytes_step * steps / (ms / 1e3) / 1e9
@@ -306,7 +339,7 @@ def run_section(args, name, stream):
            "ms_per_step": round(ms / steps, 4), "hbm_frac": round(value / peak, 4),
            "l2": ("L2 flushed (256 MB write) before every timed launch; per-launch events"
                   if flush is not None else "inputs larger than L2 (no flush)"),
-           "roofline": _roofline(plans, per_launch, steps),
+           "roofline": _roofline(plans, kind_ms, steps),
            "e2e": (run_e2e(args, plans, bufs, stream, e2e_steps=max(args.e2e_steps, 24 // len(plans)))
                    if args.e2e_steps > 0 else None),
            "clocks": clocks}
@@ -335,20 +368,27 @@ def run_ours(args, rank, world, dist):
         h.tune_cache_load(args.tune_cache)
         tiles = (f"autotune cache {os.path.relpath(args.tune_cache, ROOT)} "
                  f"({h.tune_cache_size()} entries; heuristic on a miss)")
+    if args.batched_only:
+        # the batched form alone (profiling a small batch: --batch-count)
+        pool, pool_buffers = _batch_pool(args)
+        out = {"batched": run_batched(args, stream, pool), "tiles": tiles}
+        del pool, pool_buffers
+        return out
 
     plans, bufs = _make_plans(cases, rank)
     flush = _l2_flush() if args.workload == "plain" else None
-    elapsed_ms, per_launch_ms, clocks = _timed_steps(plans, args.steps, args.warmup, stream,
-                                                     dist, world, flush=flush)
-    device_ms = sum(per_launch_ms)
+    elapsed_ms, kind_ms, clocks = _timed_steps(plans, args.steps, args.warmup, stream,
+                                               dist, world, flush=flush)
+    device_ms = sum(kind_ms.values())
     bytes_step = sum(bb for _, bb, _, _ in plans)
     value = aggregate_gbs(bytes_step * args.steps, world, elapsed_ms)
     ms_per_step = elapsed_ms / args.steps
     peak, _ = _peaks()
-    # DRAM traffic per launch: the committed per-case ncu captures of the
-    # sweep (profiles/traffic.json), as a ratio to algorithmic bytes
+    # DRAM traffic per launch: the committed single-launch ncu captures of
+    # sample sweep cases (profiles/traffic.json), as a ratio to algorithmic
+    # bytes per kernel
     ratio = _profiled_traffic() if args.workload == "sweep" and args.case is None else None
-    roofline = _roofline(plans, per_launch_ms, args.steps, ratio)
+    roofline = _roofline(plans, kind_ms, args.steps, ratio)
 
     e2e = run_e2e(args, plans, bufs, stream, dist, world) if args.e2e_steps > 0 else None
     gpu_launches = sum(p.launches for p, _, _, _ in plans) * args.steps
@@ -407,14 +447,16 @@ def run_ours(args, rank, world, dist):
 
 
 def _profiled_traffic():
-    """DRAM bytes (read + write) per algorithmic byte of the sweep's tile
-    launches, from the committed one-launch ncu captures of sample cases
-    (profiles/traffic.json; see profiles/k_tile_sweep_traffic.md)."""
+    """DRAM bytes (read + write) per algorithmic byte of each kernel, from the
+    committed single-launch ncu captures of sample sweep cases
+    (profiles/traffic.json; the captures and their command are in
+    profiles/traffic_sweep_cases.md)."""
     p = os.path.join(ROOT, "profiles", "traffic.json")
     if not os.path.exists(p):
         return None
     try:
-        return float(json.load(open(p))["dram_per_algorithmic_byte"])
+        d = json.load(open(p))
+        return {k: float(v["dram_per_algorithmic_byte"]) for k, v in d["kernels"].items()}
     except Exception:
         return None
 
@@ -933,6 +975,8 @@ def main():
     ap.add_argument("--no-batched", action="store_true",
                     help="skip the batched-form measurement")
     ap.add_argument("--batch-count", type=int, default=4096)
+    ap.add_argument("--batched-only", action="store_true",
+                    help="measure only the batched form (with --batch-count: profiling)")
     ap.add_argument("--no-served", action="store_true",
                     help="skip the served-form measurement")
     ap.add_argument("--serve-rates", default="10000,30000,100000,250000,500000")

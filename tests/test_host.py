@@ -78,3 +78,25 @@ def test_tile_invariants_random(seed):
         assert p["W"] * p["TX"] <= 256 and p["W"] * p["TY"] <= 256
         assert p["LD"] >= p["W"] * p["TX"]
         assert p["smem"] <= 227 * 1024  # opt-in shared memory per CTA on sm_100
+
+
+def test_bench_roofline_picks_the_dominant_kernel(monkeypatch, tmp_path):
+    """bench.py's roofline: the kernel kind with the most device time, its
+    algorithmic bytes over its back-to-back pass time, DRAM traffic from the
+    committed per-kernel ratio."""
+    import json
+    import bench
+    plans = [(None, 10**9, "tile", {}), (None, 2 * 10**9, "vtile", {}),
+             (None, 10**9, "rows", {})]
+    kind_ms = {"tile": 10.0, "vtile": 30.0, "rows": 5.0}   # summed over 5 steps
+    monkeypatch.setattr(bench, "_peaks", lambda: (6000.0, "measured"))
+    r = bench._roofline(plans, kind_ms, 5, {"k_vtile": 0.95, "k_tile": 1.01})
+    assert r["kernel"] == "k_vtile"
+    assert r["achieved"] == round(2e9 * 5 / 0.030 / 1e9, 1)
+    assert r["frac"] == round(r["achieved"] / 6000.0, 4)
+    assert r["traffic"] == int(2 * 10**9 * 0.95)
+    assert r["share_of_device_time"] == round(30.0 / 45.0, 4)
+    assert set(r["kernels"]) == {"k_tile", "k_vtile", "k_rows"}
+    # the committed traffic file parses into per-kernel ratios
+    t = bench._profiled_traffic()
+    assert t is None or all(0.5 < v < 2.0 for v in t.values())
