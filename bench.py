@@ -368,10 +368,15 @@ def run_ours(args, rank, world, dist):
         h.tune_cache_load(args.tune_cache)
         tiles = (f"autotune cache {os.path.relpath(args.tune_cache, ROOT)} "
                  f"({h.tune_cache_size()} entries; heuristic on a miss)")
-    if args.batched_only:
-        # the batched form alone (profiling a small batch: --batch-count)
+    if args.batched_only or args.served_only:
+        # the batched or served form alone (profiling; --batch-count,
+        # --serve-rates, --serve-seconds)
         pool, pool_buffers = _batch_pool(args)
-        out = {"batched": run_batched(args, stream, pool), "tiles": tiles}
+        out = {"tiles": tiles}
+        if args.batched_only:
+            out["batched"] = run_batched(args, stream, pool)
+        if args.served_only:
+            out["served"] = run_served(args, pool)
         del pool, pool_buffers
         return out
 
@@ -977,6 +982,8 @@ def main():
     ap.add_argument("--batch-count", type=int, default=4096)
     ap.add_argument("--batched-only", action="store_true",
                     help="measure only the batched form (with --batch-count: profiling)")
+    ap.add_argument("--served-only", action="store_true",
+                    help="measure only the served form (--serve-rates, --serve-seconds)")
     ap.add_argument("--no-served", action="store_true",
                     help="skip the served-form measurement")
     ap.add_argument("--serve-rates", default="10000,30000,100000,250000,500000")

@@ -9,12 +9,18 @@
 //     budget; a request whose output buffer an earlier unfinished request
 //     still writes waits in that buffer's own queue (and does not hold up
 //     later ones): admission is constant time per request;
-//   * batched mode: packs the admitted requests of one pass (at most
-//     max_batch) into one launch -- the batch layout and group kernels of the
-//     batched form -- on the next free stream of a pool of
-//     max_inflight_launches streams, so requests that arrive while earlier
-//     launches run are admitted into new launches that overlap them on the
-//     device;
+//   * batched mode, light load (no batched launch in flight, at most
+//     kPlainReady requests ready): each request runs as its own plain exec
+//     on the least loaded of kPlainStreams streams (up to kPlainSlots in
+//     flight), so a lone request costs one kernel launch, as in the per-call
+//     loop, and small requests overlap;
+//   * batched mode, backlog: packs the admitted requests of one pass (at
+//     most max_batch, and at most kBatchBytes algorithmic bytes, so one
+//     launch does not hold the queue for milliseconds) into one launch -- the
+//     batch layout and group kernels of the batched form -- on the next free
+//     stream of a pool of max_inflight_launches streams, so requests that
+//     arrive while earlier launches run are admitted into new launches that
+//     overlap them on the device;
 //   * per-call mode (the baseline): one plain exec per request, in arrival
 //     order, on one stream;
 //   * notices completions by polling each launch's event, stamps every
@@ -65,6 +71,21 @@ struct Request {
 // on the shared stream).
 constexpr int kAuxStreams = 3;
 constexpr size_t kForkMinRequests = 32;
+// Light-load plain execs (batched mode): streams, launches in flight, and the
+// most requests ready for which the scheduler still runs them one by one.
+// Measured at 10k-100k req/s on the mixed pool: batching a pass of two or
+// three requests (layout upload, several group kernels) doubled p99 against
+// one plain exec per request; a backlog beyond a few requests is cheaper
+// batched.
+// Plain execs run only while no batched launch is in flight (the device is
+// nearly idle); under load every pass batches.  At 10k/100k/250k req/s this
+// measured p99 31/44/408 us against 57/123/539 us when every pass batched.
+constexpr int kPlainStreams = 4;
+constexpr size_t kPlainSlots = 16;
+constexpr size_t kPlainReady = 8;
+// Algorithmic bytes one batched launch takes at most (~1 ms of device time):
+// a cap of 1 GiB made launches too small to keep up at 500k req/s.
+constexpr uint64_t kBatchBytes = 4ull << 30;
 
 struct Launch {
   cudaStream_t stream = nullptr;
@@ -119,6 +140,13 @@ struct Server {
   std::vector<Launch> slots;
   std::vector<size_t> free_slots;        // indices of idle slots
   std::deque<size_t> inflight;           // busy slots in launch order
+  // light-load plain execs (batched mode): one request each, on the plain
+  // streams; each stream's launches finish in order, so only the head of its
+  // FIFO is polled
+  std::vector<Launch> plain;
+  std::vector<size_t> free_plain;
+  cudaStream_t plain_stream[kPlainStreams] = {};
+  std::deque<size_t> plain_fifo[kPlainStreams];
   cudaStream_t shared_stream = nullptr;  // per-call mode
   std::unordered_set<const void *> claimed;
   uint64_t inflight_bytes = 0;
@@ -276,11 +304,14 @@ void enqueue_request(Server *s, const Request &r) {
 
 // Admit ready requests into launch L in arrival order while they fit the
 // budget.  Returns the number admitted.
-size_t admit(Server *s, Launch *L, size_t max_n) {
+size_t admit(Server *s, Launch *L, size_t max_n, uint64_t max_alg_bytes) {
   size_t taken = 0;
+  uint64_t alg = 0;
   while (taken < max_n && !s->ready.empty()) {
     const Request &r = s->ready.front();
     if (s->inflight_bytes + r.dev_bytes > s->cfg.budget_bytes) break;
+    if (taken > 0 && alg + r.alg_bytes > max_alg_bytes) break;
+    alg += r.alg_bytes;
     s->inflight_bytes += r.dev_bytes;
     L->reqs.push_back(r);
     s->ready.pop_front();
@@ -326,7 +357,21 @@ void worker_main(Server *s) {
       fail_queued(s);
     }
     // completions: per-call launches share one stream and finish in order,
-    // so only the oldest is polled; batched launches (a few streams) each
+    // so only the oldest is polled; light-load plain execs likewise per
+    // plain stream; batched launches (a few streams) each
+    for (int q = 0; q < kPlainStreams; ++q) {
+      auto &fifo = s->plain_fifo[q];
+      while (!fifo.empty()) {
+        Launch &L = s->plain[fifo.front()];
+        const cudaError_t e = cudaEventQuery(L.done);
+        if (e == cudaErrorNotReady) break;
+        if (e != cudaSuccess) cudaGetLastError();
+        finish_launch(s, &L, e == cudaSuccess ? ST_OK : ST_CUDA);
+        s->free_plain.push_back(fifo.front());
+        fifo.pop_front();
+        progress = true;
+      }
+    }
     for (auto it = s->inflight.begin(); it != s->inflight.end();) {
       Launch &L = s->slots[*it];
       const cudaError_t q = cudaEventQuery(L.done);
@@ -341,11 +386,40 @@ void worker_main(Server *s) {
       it = s->inflight.erase(it);
       progress = true;
     }
-    // admissions: every idle slot takes the next admissible requests
+    // admissions, light load: one plain exec per request while few are
+    // ready, on the plain stream with the fewest launches in flight
+    while (!s->cfg.per_call && s->inflight.empty() && !s->ready.empty() &&
+           s->ready.size() <= kPlainReady && !s->free_plain.empty()) {
+      int q = 0;
+      for (int i = 1; i < kPlainStreams; ++i)
+        if (s->plain_fifo[i].size() < s->plain_fifo[q].size()) q = i;
+      const size_t k = s->free_plain.back();
+      Launch &L = s->plain[k];
+      L.stream = s->plain_stream[q];
+      if (admit(s, &L, 1, kBatchBytes) == 0) break;
+      s->free_plain.pop_back();
+      {
+        std::lock_guard<std::mutex> lk(s->mu);
+        s->peak_inflight_bytes = std::max(s->peak_inflight_bytes, s->inflight_bytes);
+        ++s->launches;
+        s->batched_requests += 1;
+      }
+      L.busy = true;
+      const int st = enqueue_launch(s, &L);
+      if (st != ST_OK) {
+        cudaGetLastError();
+        finish_launch(s, &L, st);
+        s->free_plain.push_back(k);
+      } else {
+        s->plain_fifo[q].push_back(k);
+      }
+      progress = true;
+    }
+    // admissions, backlog: every idle slot takes the next admissible requests
     while (!s->free_slots.empty() && !s->ready.empty()) {
       const size_t k = s->free_slots.back();
       Launch &L = s->slots[k];
-      if (admit(s, &L, max_batch) == 0) break;
+      if (admit(s, &L, max_batch, s->cfg.per_call ? ~0ull : kBatchBytes) == 0) break;
       s->free_slots.pop_back();
       {
         std::lock_guard<std::mutex> lk(s->mu);
@@ -366,7 +440,8 @@ void worker_main(Server *s) {
     }
     if (progress) continue;
     std::unique_lock<std::mutex> lk(s->mu);
-    const bool busy = !s->inflight.empty();
+    bool busy = !s->inflight.empty();
+    for (int q = 0; q < kPlainStreams; ++q) busy = busy || !s->plain_fifo[q].empty();
     if (s->stop && s->incoming.empty() && s->ready.empty() && s->n_waiting == 0 && !busy)
       break;
     if (!busy && s->incoming.empty()) {
@@ -395,6 +470,13 @@ void free_slots(Server *s) {
     if (L.h_work) cudaFreeHost(L.h_work);
   }
   s->slots.clear();
+  for (Launch &L : s->plain)
+    if (L.done) cudaEventDestroy(L.done);
+  s->plain.clear();
+  for (int q = 0; q < kPlainStreams; ++q) {
+    if (s->plain_stream[q]) cudaStreamDestroy(s->plain_stream[q]);
+    s->plain_stream[q] = nullptr;
+  }
   if (s->shared_stream) cudaStreamDestroy(s->shared_stream);
   s->shared_stream = nullptr;
 }
@@ -449,6 +531,16 @@ int hptt_cuda_server_create(const hptt_cuda_serve_config *cfg, hptt_cuda_server_
             cudaEventCreateWithFlags(&L.join[k], cudaEventDisableTiming) != cudaSuccess)
           st = ST_CUDA;
     }
+  }
+  if (!cfg->per_call) {
+    for (int q = 0; q < kPlainStreams && st == ST_OK; ++q)
+      if (cudaStreamCreateWithFlags(&s->plain_stream[q], cudaStreamNonBlocking) != cudaSuccess)
+        st = ST_CUDA;
+    s->plain.resize(kPlainSlots);
+    for (Launch &L : s->plain)
+      if (st == ST_OK && cudaEventCreateWithFlags(&L.done, cudaEventDisableTiming) != cudaSuccess)
+        st = ST_CUDA;
+    for (size_t k = s->plain.size(); k-- > 0;) s->free_plain.push_back(k);
   }
   if (st != ST_OK) {
     cudaGetLastError();
