@@ -474,7 +474,9 @@ def run_e2e(args, plans, bufs, stream, dist=None, world=1, e2e_steps=None):
     runs exec, and copies B back to pinned host memory.  Transposes rotate
     over three streams with one staging pair each, so one transpose's
     host->device copy overlaps the previous ones' kernels and device->host
-    copies (PCIe is full duplex) without waiting for a staging pair."""
+    copies (PCIe is full duplex) without waiting for a staging pair; the
+    rotation continues across steps, so with one transpose per step (the
+    plain workload) a step's upload overlaps the previous step's download."""
     import torch
     host = {}
     for key, (a, b) in bufs.items():
@@ -499,8 +501,13 @@ def run_e2e(args, plans, bufs, stream, dist=None, world=1, e2e_steps=None):
         d2h += nbytes
         work.append((p, key, nbytes, reads_b, a.dtype))
 
+    issued = [0]  # transposes issued so far: consecutive ones, also across
+                  # steps, go to different streams and staging pairs
+
     def step():
-        for i, (p, key, nbytes, reads_b, dt) in enumerate(work):
+        for p, key, nbytes, reads_b, dt in work:
+            i = issued[0]
+            issued[0] += 1
             s = streams[i % len(streams)]
             sa, sb, hout = stage[i % len(streams)]
             ha, hb = host[key]

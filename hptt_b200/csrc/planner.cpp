@@ -555,19 +555,20 @@ int vtile_bank_cost(const HpttTile &t, int ld, int sz, const std::vector<int64_t
   const int warps = std::min(t.nt / 32, 8);
   for (int w = 0; w < warps; ++w) {
     for (int i = 0; i < V; ++i) {
+      // load phase: the warp's first rows, first slot group
       for (int l = 0; l < 32; ++l) {
-        const dev::VtPos ps = dev::vt_pos(w * 32 + l, t.vlx);
+        const dev::VtPos ps = dev::vt_pos(w * 32 + l);
         const int y = ps.r0;
         addr[l] = -1;
         if (y >= t.TY) continue;
         const int sh = md(rowA[y]);
-        const int x = ps.k * V - sh + i;
         if (ps.k * V - sh >= t.TX) continue;
-        addr[l] = (static_cast<int64_t>(y + P) * ld + x + P) * sz;
+        addr[l] = (static_cast<int64_t>(y + P) * ld + ps.k * V - sh + i + P) * sz;
       }
       cost += excess_wavefronts(addr, 32, sz);
+      // store phase: the warp's first columns, first slot group
       for (int l = 0; l < 32; ++l) {
-        const dev::VtPos ps = dev::vt_pos(w * 32 + l, t.vly);
+        const dev::VtPos ps = dev::vt_pos(w * 32 + l);
         const int x = ps.r0;
         addr[l] = -1;
         if (x >= t.TX) continue;
@@ -602,12 +603,17 @@ int choose_vtile(const HpttProblem &p, const TileParams &tp, HpttTile *t) {
   t->xc = t->yc = t->wc = -1;
   auto fits = [](int n) { return n == 8 || n == 16 || n == 32; };
   if (!fits(tp.vt_nvx) || !fits(tp.vt_nvy)) return ST_TOO_LARGE;
-  if (tp.nt / tp.vt_nvx < 4 || tp.nt / tp.vt_nvy < 4) return ST_TOO_LARGE;
+  if (tp.nt != 256 && tp.nt != 512) return ST_TOO_LARGE;
+  // lines (rows in the load phase, columns in the store phase) per pass: a
+  // warp covers 4, each thread every eighth window slot of its lines, so a
+  // thread holds J lines x (slots / 8) vectors
+  const int R = tp.nt / 8;
   bool in_x[HPTT_MAX_RANK] = {false};
   int64_t tile_ext[HPTT_MAX_RANK];
   for (int d = 0; d < r; ++d) tile_ext[d] = 1;
   // X run: bounded by the load window and by the store phase's iterations
-  const int64_t txmax = std::min<int64_t>(tp.vt_nvx * V - V + 1, (tp.nt / tp.vt_nvy) * JV);
+  const int64_t txmax =
+      std::min<int64_t>(tp.vt_nvx * V - V + 1, static_cast<int64_t>(R) * (JV / (tp.vt_nvy / 8)));
   int64_t TX = 1;
   for (int d = 0; d < r; ++d) {
     if (d == p.perm[0]) break;
@@ -634,8 +640,9 @@ int choose_vtile(const HpttProblem &p, const TileParams &tp, HpttTile *t) {
   // fewest load slots that cover the run
   int nvx = 8;
   while (nvx * V - V + 1 < TX) nvx *= 2;
-  const int R1 = tp.nt / nvx;
-  const int64_t tymax = std::min<int64_t>(tp.vt_nvy * V - V + 1, static_cast<int64_t>(R1) * JV);
+  const int R1 = R;
+  const int64_t tymax =
+      std::min<int64_t>(tp.vt_nvy * V - V + 1, static_cast<int64_t>(R1) * (JV / (nvx / 8)));
   int64_t TY = 1;
   for (int k = 0; k < r; ++k) {
     const int d = p.perm[k];
@@ -660,8 +667,8 @@ int choose_vtile(const HpttProblem &p, const TileParams &tp, HpttTile *t) {
   if (t->ny == 0) return ST_TOO_LARGE;
   int nvy = 8;
   while (nvy * V - V + 1 < TY) nvy *= 2;
-  const int R2 = tp.nt / nvy;
-  if (cdiv(TY, R1) > JV || cdiv(TX, R2) > JV) return ST_TOO_LARGE;
+  const int R2 = R;
+  if (cdiv(TY, R1) * (nvx / 8) > JV || cdiv(TX, R2) * (nvy / 8) > JV) return ST_TOO_LARGE;
   t->vlx = log2_slots(nvx);
   t->vly = log2_slots(nvy);
   t->TX = static_cast<int32_t>(TX);

@@ -328,9 +328,12 @@ int replay_vtile(const HpttProblem &P, const HpttTile &T, int update, const Layo
   const int V = 16 / esz, PD = V - 1;
   const int JV = hptt_vt_jmax();
   if (V < 2) return 301;
-  if (T.J1 > JV || T.J2 > JV) return 302;
   const int nvx = 8 << T.vlx, nvy = 8 << T.vly;
-  if (T.R1 != T.nt / nvx || T.R2 != T.nt / nvy) return 303;
+  const int GX = nvx / 8, GY = nvy / 8;  // slots of a line a thread takes
+  // vectors a thread holds: J lines x slot groups, within the kernel's
+  // compile-time limit
+  if (T.J1 * GX > JV || T.J2 * GY > JV) return 302;
+  if (T.R1 != T.nt / 8 || T.R2 != T.nt / 8) return 303;
   if (T.R1 * T.J1 < T.TY || T.R2 * T.J2 < T.TX) return 304;
   if (nvx * V - PD < T.TX || nvy * V - PD < T.TY) return 305;
   if (T.LD < nvx * V + PD) return 306;
@@ -364,40 +367,48 @@ int replay_vtile(const HpttProblem &P, const HpttTile &T, int update, const Layo
     if (limX < 1 || limY < 1 || limX > T.TX || limY > T.TY) return 314;
     std::fill(slot.begin(), slot.end(), -1);
     for (int t = 0; t < T.nt; ++t) {
-      const VtPos ps = vt_pos(t, T.vlx);
-      if (ps.k >= nvx || ps.r0 >= T.R1) return 315;
-      const int xk = ps.k * V;
-      for (int j = 0; j < JV; ++j) {
+      const VtPos ps = vt_pos(t);
+      if (ps.k >= 8 || ps.r0 >= T.R1) return 315;
+      for (int j = 0; j < T.J1; ++j) {
         const int y = ps.r0 + j * T.R1;
-        if (!(j < T.J1 && y < limY)) continue;
+        if (!(y < limY)) continue;
         const int64_t row = o.bA + static_cast<int64_t>(tabY[y]);  // element index in A
         const int sh = md(misA + row);
-        if (!(xk - sh < limX)) continue;
-        const int64_t w = row - sh + xk;
-        if (md(misA + w) != 0) return 316;        // 16-byte aligned window
-        if (!window_ok(w, L.nA)) return 317;     // inside the buffer's blocks
-        for (int i = 0; i < V; ++i) {
-          const int x = xk - sh + i;
-          const int64_t si = static_cast<int64_t>(y + PD) * T.LD + x + PD;
-          if (si < 0 || si >= smem_elems) return 318;
-          if (x < 0 || x >= limX) continue;      // padding, never read
-          if (slot[si] >= 0) return 319;         // two writers of one slot
-          const int64_t ia = w + i;
-          if (ia < 0 || ia >= L.nA) return 320;
-          if (ia != row + x) return 321;
-          slot[si] = ia;
+        for (int g = 0; g < GX; ++g) {
+          const int xk = (ps.k + 8 * g) * V;
+          // every window of the row goes to shared memory (read or not)
+          for (int i = 0; i < V; ++i) {
+            const int64_t si = static_cast<int64_t>(y + PD) * T.LD + xk - sh + i + PD;
+            if (si < 0 || si >= smem_elems) return 318;
+            if (si / T.LD != y + PD) return 331;   // stays inside its own row
+          }
+          if (!(xk - sh < limX)) continue;           // not read
+          const int64_t w = row - sh + xk;
+          if (md(misA + w) != 0) return 316;        // 16-byte aligned window
+          if (!window_ok(w, L.nA)) return 317;     // inside the buffer's blocks
+          for (int i = 0; i < V; ++i) {
+            const int x = xk - sh + i;
+            const int64_t si = static_cast<int64_t>(y + PD) * T.LD + x + PD;
+            if (x < 0 || x >= limX) continue;      // padding, never read
+            if (slot[si] >= 0) return 319;         // two writers of one slot
+            const int64_t ia = w + i;
+            if (ia < 0 || ia >= L.nA) return 320;
+            if (ia != row + x) return 321;
+            slot[si] = ia;
+          }
         }
       }
     }
     for (int t = 0; t < T.nt; ++t) {
-      const VtPos ps = vt_pos(t, T.vly);
-      if (ps.k >= nvy || ps.r0 >= T.R2) return 322;
-      const int yk = ps.k * V;
-      for (int j = 0; j < JV; ++j) {
+      const VtPos ps = vt_pos(t);
+      if (ps.k >= 8 || ps.r0 >= T.R2) return 322;
+      for (int j = 0; j < T.J2; ++j) {
         const int x = ps.r0 + j * T.R2;
-        if (!(j < T.J2 && x < limX)) continue;
+        if (!(x < limX)) continue;
         const int64_t col = o.bB + static_cast<int64_t>(tabX[x]);  // element index in B
         const int tt = md(misB + col);
+        for (int g = 0; g < GY; ++g) {
+        const int yk = (ps.k + 8 * g) * V;
         const int y0 = yk - tt;
         if (!(y0 < limY)) continue;
         const int64_t w = col - tt + yk;
@@ -420,6 +431,7 @@ int replay_vtile(const HpttProblem &P, const HpttTile &T, int update, const Layo
           ++*checked;
         }
         (void)full;
+        }
       }
     }
   }

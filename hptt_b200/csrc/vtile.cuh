@@ -29,9 +29,10 @@
 //                by one.  When B is read, the B window is read whole first
 //                (same 16-byte-block argument) and only its column's
 //                elements are written back.
-// Thread mapping: a warp covers 8 consecutive window slots of 4 rows (load)
-// or of 4 columns (store): every global access of a warp is four 128-byte
-// runs, and the host picks the row pitch LD that minimises shared-memory
+// Thread mapping (vt_pos): a warp covers 8 consecutive window slots of 4
+// rows (load) or of 4 columns (store), so every global access of a warp is
+// four 128-byte runs; a thread walks every eighth slot of its rows or
+// columns.  The host picks the row pitch LD that minimises shared-memory
 // bank conflicts of exactly these accesses (vtile_bank_cost).
 //
 // This replaces the reference's 256-bit in-register micro kernels
@@ -52,18 +53,19 @@ namespace dev {
 // Vector loads (rows) or stores (columns) a thread keeps in flight per phase.
 HPTT_HD constexpr int hptt_vt_jmax() { return 8; }
 
-// Thread `tid` -> (window slot k along a line, first line r0) of one phase;
-// lines r0 + j * (nt >> (3 + lg)).  A warp holds 8 slots of 4 lines; a line
-// has 8 << lg slots.
+// Thread `tid` -> (first window slot k of its lines, first line r0) of
+// either phase: a warp holds 8 consecutive slots of 4 lines (4 * 128 bytes
+// per access); a thread takes slots k, k + 8, ... of each of its lines, and
+// lines r0 + j * (nt / 8).  So a line's offset and window shift are worked
+// out once per thread and line, not once per vector.
 struct VtPos {
   int k, r0;
 };
 
-HPTT_HD inline VtPos vt_pos(int tid, int lg) {
-  const int w = tid >> 5;
+HPTT_HD inline VtPos vt_pos(int tid) {
   VtPos p;
-  p.k = (tid & 7) | ((w & ((1 << lg) - 1)) << 3);
-  p.r0 = ((tid >> 3) & 3) | ((w >> lg) << 2);
+  p.k = tid & 7;
+  p.r0 = ((tid >> 5) << 2) | ((tid >> 3) & 3);
   return p;
 }
 
@@ -95,102 +97,111 @@ __device__ __forceinline__ int vt_shift(const E *p) {
   return static_cast<int>((reinterpret_cast<uintptr_t>(p) / sizeof(E)) & (V - 1));
 }
 
-template <typename E, int MODE, bool UPD, typename OffT, bool LX, bool LY>
-__device__ __forceinline__ void vtile_one(const HpttProblem &P, const HpttTile &T,
-                                          const E *__restrict__ A, E *__restrict__ B,
-                                          const unsigned char *__restrict__ tables,
-                                          const Op<E, MODE, UPD> &op, E *sdata,
-                                          uint32_t tile) {
+// Load phase: rows of A into shared memory.  Thread (k, r0) reads window
+// slots k + 8 g (g < G = 8 slots groups of a row) of rows r0 + j * R1.  A
+// row's offset steps by R1 * sya (one Y dim) or comes from the table; its
+// window shift is (shift of the tile origin + row offset) mod V.  Every
+// window of a row below limY goes to shared memory whole: a window that was
+// not read (it starts at or past limX) lands in the row's padding.
+template <typename E, typename OffT, bool LY, int LG>
+__device__ __forceinline__ void vt_load(const HpttTile &T, const E *__restrict__ a0,
+                                        const OffT *__restrict__ tabY, E *sm, int limX,
+                                        int limY) {
   constexpr int V = 16 / sizeof(E);
-  constexpr int JV = hptt_vt_jmax();
+  constexpr int G = 1 << LG;
   using VecT = Vec<E, V>;
-  static_assert(sizeof(VecT) == 16, "16-byte vectors");
-  const TileOrigin o = tile_origin(P, T, tile);
-  const int limX = vt_lim_x(T, o), limY = vt_lim_y(T, o);
+  const VtPos ps = vt_pos(threadIdx.x);
+  const int xk = ps.k * V;
+  const int R1 = T.R1;
+  const int s0 = vt_shift(a0);
   const int LD = T.LD;
-  E *sm = sdata + (V - 1) * (LD + 1);
-  const OffT *__restrict__ tabY = reinterpret_cast<const OffT *>(tables);
-  const OffT *__restrict__ tabX = reinterpret_cast<const OffT *>(tables + T.tab2_off);
-  // ---- load phase: rows of A into shared memory ----
-  // Thread (k, r0) reads window slot k of rows r0 + j * R1.  A row's offset
-  // steps by R1 * sya (one Y dim) or comes from the table; its window shift
-  // is (shift of the tile origin + row offset) mod V.
-  {
-    const VtPos ps = vt_pos(threadIdx.x, T.vlx);
-    const int xk = ps.k * V;
-    const int R1 = T.R1;
-    const E *a0 = A + o.bA;
-    const int s0 = vt_shift(a0);
+  with_trip_count<hptt_vt_jmax() / G>(T.J1, [&](auto nn) {
+    constexpr int N = decltype(nn)::value;
+    VecT v[N][G];
+    int sh[N];
+    OffT off = LY ? static_cast<OffT>(ps.r0) * static_cast<OffT>(T.sya) : OffT(0);
     const OffT stepA = LY ? static_cast<OffT>(R1) * static_cast<OffT>(T.sya) : OffT(0);
-    E *srow = sm + ps.r0 * LD + xk;
-    const int sstep = R1 * LD;
-    with_trip_count<JV>(T.J1, [&](auto nn) {
-      constexpr int N = decltype(nn)::value;
-      VecT v[N];
-      int sh[N];
-      OffT off = LY ? static_cast<OffT>(ps.r0) * static_cast<OffT>(T.sya) : OffT(0);
 #pragma unroll
-      for (int j = 0; j < N; ++j) {
-        const int y = ps.r0 + j * R1;
-        if (!LY) off = tabY[min(y, T.TY - 1)];
-        const int s = (s0 + static_cast<int>(off)) & (V - 1);
-        sh[j] = (y < limY && xk - s < limX) ? s : -1;
-        if (sh[j] >= 0) v[j] = ld_vec<E, V>(a0 + static_cast<int64_t>(off) + (xk - s));
-        if (LY) off += stepA;
+    for (int j = 0; j < N; ++j) {
+      const int y = ps.r0 + j * R1;
+      if (!LY) off = tabY[min(y, T.TY - 1)];
+      const int s = (s0 + static_cast<int>(off)) & (V - 1);
+      sh[j] = y < limY ? s : -1;
+      const E *w = a0 + static_cast<int64_t>(off) + (xk - s);
+#pragma unroll
+      for (int g = 0; g < G; ++g)
+        if (sh[j] >= 0 && xk + 8 * V * g - s < limX) v[j][g] = ld_vec<E, V>(w + 8 * V * g);
+      if (LY) off += stepA;
+    }
+#pragma unroll
+    for (int j = 0; j < N; ++j) {
+      if (sh[j] >= 0) {
+        E *d = sm + (ps.r0 + j * R1) * LD + xk - sh[j];
+#pragma unroll
+        for (int g = 0; g < G; ++g)
+#pragma unroll
+          for (int i = 0; i < V; ++i) d[8 * V * g + i] = v[j][g].v[i];
       }
-#pragma unroll
-      for (int j = 0; j < N; ++j) {
-        if (sh[j] >= 0) {
-          E *d = srow + j * sstep - sh[j];
-#pragma unroll
-          for (int i = 0; i < V; ++i) d[i] = v[j].v[i];
-        }
-      }
-    });
-  }
-  __syncthreads();
-  // ---- store phase: columns of B from shared memory ----
-  // Thread (k, c0) writes window slot k of columns c0 + j * R2: element y of
-  // the slot is y0 + i with y0 = V * k - t (t = the column's window shift).
-  const VtPos ps = vt_pos(threadIdx.x, T.vly);
+    }
+  });
+}
+
+// Store phase: columns of B from shared memory.  Thread (k, c0) writes window
+// slots k + 8 g of columns c0 + j * R2; slot element i is y = V (k + 8 g) - t
+// + i, t the column's window shift.  When B is read, all of the thread's B
+// windows are read first.
+template <typename E, int MODE, bool UPD, typename OffT, bool LX, int LG>
+__device__ __forceinline__ void vt_store(const HpttTile &T, E *__restrict__ b0,
+                                         const OffT *__restrict__ tabX, const E *sm,
+                                         const Op<E, MODE, UPD> &op, int limX, int limY) {
+  constexpr int V = 16 / sizeof(E);
+  constexpr int G = 1 << LG;
+  using VecT = Vec<E, V>;
+  const VtPos ps = vt_pos(threadIdx.x);
   const int yk = ps.k * V;
   const int R2 = T.R2;
-  E *b0 = B + o.bB;
   const int t0 = vt_shift(b0);
-  const E *scol = sm + yk * LD + ps.r0;
-  with_trip_count<JV>(T.J2, [&](auto nn) {
+  const int LD = T.LD;
+  with_trip_count<hptt_vt_jmax() / G>(T.J2, [&](auto nn) {
     constexpr int N = decltype(nn)::value;
-    // column j's offset and window shift (-1: nothing of it in this slot)
+    // column j's offset and window shift (-1: outside the tile)
     auto column = [&](int j, OffT &off) -> int {
       const int x = ps.r0 + j * R2;
       off = LX ? static_cast<OffT>(x) * static_cast<OffT>(T.sxb) : tabX[min(x, T.TX - 1)];
       const int t = (t0 + static_cast<int>(off)) & (V - 1);
-      return (x < limX && yk - t < limY) ? t : -1;
+      return x < limX ? t : -1;
     };
-    VecT bv[UPD ? N : 1];
+    VecT bv[UPD ? N : 1][UPD ? G : 1];
     if (UPD) {
-      // the B windows first, all in flight together
 #pragma unroll
       for (int j = 0; j < N; ++j) {
         OffT off;
         const int t = column(j, off);
-        if (t >= 0) bv[UPD ? j : 0] = ld_vec_rw<E, V>(b0 + static_cast<int64_t>(off) + (yk - t));
+        const E *w = b0 + static_cast<int64_t>(off) + (yk - t);
+#pragma unroll
+        for (int g = 0; g < G; ++g)
+          if (t >= 0 && yk + 8 * V * g - t < limY)
+            bv[UPD ? j : 0][UPD ? g : 0] = ld_vec_rw<E, V>(w + 8 * V * g);
       }
     }
 #pragma unroll
     for (int j = 0; j < N; ++j) {
       OffT off;
       const int t = column(j, off);
-      if (t >= 0) {
-        const E *s = scol + j * R2 - t * LD;
+      if (t < 0) continue;
+      const E *s = sm + (yk - t) * LD + ps.r0 + j * R2;
+      E *w = b0 + static_cast<int64_t>(off) + (yk - t);
+#pragma unroll
+      for (int g = 0; g < G; ++g) {
+        const int y0 = yk + 8 * V * g - t;
+        if (y0 >= limY) continue;
         VecT r;
 #pragma unroll
         for (int i = 0; i < V; ++i) {
-          const E a = s[i * LD];
-          r.v[i] = op(a, UPD ? bv[UPD ? j : 0].v[i] : a);
+          const E a = s[(8 * V * g + i) * LD];
+          r.v[i] = op(a, UPD ? bv[UPD ? j : 0][UPD ? g : 0].v[i] : a);
         }
-        E *dst = b0 + static_cast<int64_t>(off) + (yk - t);
-        const int y0 = yk - t;
+        E *dst = w + 8 * V * g;
         if (y0 >= 0 && y0 + V <= limY) {
           if (UPD)
             st_vec<E, V>(dst, r);
@@ -210,6 +221,36 @@ __device__ __forceinline__ void vtile_one(const HpttProblem &P, const HpttTile &
       }
     }
   });
+}
+
+template <typename E, int MODE, bool UPD, typename OffT, bool LX, bool LY>
+__device__ __forceinline__ void vtile_one(const HpttProblem &P, const HpttTile &T,
+                                          const E *__restrict__ A, E *__restrict__ B,
+                                          const unsigned char *__restrict__ tables,
+                                          const Op<E, MODE, UPD> &op, E *sdata,
+                                          uint32_t tile) {
+  constexpr int V = 16 / sizeof(E);
+  static_assert(sizeof(Vec<E, V>) == 16, "16-byte vectors");
+  const TileOrigin o = tile_origin(P, T, tile);
+  const int limX = vt_lim_x(T, o), limY = vt_lim_y(T, o);
+  E *sm = sdata + (V - 1) * (T.LD + 1);
+  const OffT *__restrict__ tabY = reinterpret_cast<const OffT *>(tables);
+  const OffT *__restrict__ tabX = reinterpret_cast<const OffT *>(tables + T.tab2_off);
+  const E *a0 = A + o.bA;
+  if (T.vlx == 0)
+    vt_load<E, OffT, LY, 0>(T, a0, tabY, sm, limX, limY);
+  else if (T.vlx == 1)
+    vt_load<E, OffT, LY, 1>(T, a0, tabY, sm, limX, limY);
+  else
+    vt_load<E, OffT, LY, 2>(T, a0, tabY, sm, limX, limY);
+  __syncthreads();
+  E *b0 = B + o.bB;
+  if (T.vly == 0)
+    vt_store<E, MODE, UPD, OffT, LX, 0>(T, b0, tabX, sm, op, limX, limY);
+  else if (T.vly == 1)
+    vt_store<E, MODE, UPD, OffT, LX, 1>(T, b0, tabX, sm, op, limX, limY);
+  else
+    vt_store<E, MODE, UPD, OffT, LX, 2>(T, b0, tabX, sm, op, limX, limY);
 }
 
 }  // namespace dev
