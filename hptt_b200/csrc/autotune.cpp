@@ -39,9 +39,9 @@ const char *env_path() { return std::getenv("HPTT_B200_TUNE_CACHE"); }
 
 // Cache file: one line per key,
 // "key|run vmin smem rows_min y_first iters full_side walk upd_exact nt
-//  grid_order vt vt_nvx vt_nvy"
+//  grid_order vt vt_nvx vt_nvy vt_j"
 // (missing trailing fields read as 0, walk and upd_exact as 1, nt as 256,
-// vt_nvx and vt_nvy as 16).
+// vt_nvx and vt_nvy as 16, vt_j as 8).
 void read_cache_stream(std::istream &f) {
   std::string line;
   while (std::getline(f, line)) {
@@ -60,6 +60,7 @@ void read_cache_stream(std::istream &f) {
       if (!(v >> tp.vt)) tp.vt = 0;
       if (!(v >> tp.vt_nvx)) tp.vt_nvx = 16;
       if (!(v >> tp.vt_nvy)) tp.vt_nvy = 16;
+      if (!(v >> tp.vt_j) || (tp.vt_j != 4 && tp.vt_j != 8)) tp.vt_j = 8;
       g_cache[line.substr(0, bar)] = tp;
     }
   }
@@ -83,7 +84,7 @@ int write_cache(const char *path) {
       << kv.second.y_first << " " << kv.second.max_iters << " " << kv.second.full_side << " "
       << kv.second.walk << " " << kv.second.upd_exact << " " << kv.second.nt << " "
       << kv.second.grid_order << " " << kv.second.vt << " " << kv.second.vt_nvx << " "
-      << kv.second.vt_nvy << "\n";
+      << kv.second.vt_nvy << " " << kv.second.vt_j << "\n";
   return ST_OK;
 }
 
@@ -96,20 +97,22 @@ std::vector<TileParams> candidates(const HpttProblem &prob) {
   const int elem_size = elem_bytes(prob.dtype);
   std::vector<TileParams> c;
   // vector tiles first (window slots per row and per column, threads per
-  // CTA, grid order), where the shape allows one
+  // CTA, vectors per thread, grid order), where the shape allows one
   if (vtile_possible(prob))
-    for (int nt : {256, 512})
-      for (int nvx : {8, 16, 32})
-        for (int nvy : {8, 16, 32})
-          for (int go : {0, 1}) {
-            TileParams tp;
-            tp.vt = 1;
-            tp.nt = nt;
-            tp.vt_nvx = nvx;
-            tp.vt_nvy = nvy;
-            tp.grid_order = go;
-            c.push_back(tp);
-          }
+    for (int vj : {8, 4})
+      for (int nt : {256, 512})
+        for (int nvx : {8, 16, 32})
+          for (int nvy : {8, 16, 32})
+            for (int go : {0, 1}) {
+              TileParams tp;
+              tp.vt = 1;
+              tp.vt_j = vj;
+              tp.nt = nt;
+              tp.vt_nvx = nvx;
+              tp.vt_nvy = nvy;
+              tp.grid_order = go;
+              c.push_back(tp);
+            }
   for (int full : {0, 1, 2})
     for (int iters : {0, hptt_jmax_tile(elem_size) / 2})
       for (int yf : {0, 1})

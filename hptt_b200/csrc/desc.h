@@ -137,8 +137,10 @@ struct HpttTile {
   HpttWalk wx, wy;
   // KIND_VTILE: log2 of the 8-slot groups along a row of the load phase
   // (vlx) and along a column of the store phase (vly); a row has 8 << vlx
-  // vector slots, a column 8 << vly
-  int32_t vlx, vly;
+  // vector slots, a column 8 << vly; vj = the most 16-byte vectors a thread
+  // holds per phase (4 or 8: two kernel builds with their own register
+  // budgets)
+  int32_t vlx, vly, vj;
 };
 
 // One slot of a KIND_TILE offset table (OffT = uint32_t or int64_t).

@@ -593,10 +593,13 @@ int log2_slots(int n) { return n >= 32 ? 2 : (n >= 16 ? 1 : 0); }
 int choose_vtile(const HpttProblem &p, const TileParams &tp, HpttTile *t) {
   const int sz = elem_bytes(p.dtype);
   if (!vtile_possible(p)) return ST_TOO_LARGE;
-  const int V = 16 / sz, JV = dev::hptt_vt_jmax();
+  const int V = 16 / sz;
+  if (tp.vt_j != 4 && tp.vt_j != 8) return ST_TOO_LARGE;
+  const int JV = tp.vt_j;
   const int r = p.rank;
   std::memset(t, 0, sizeof(*t));
   t->kind = KIND_VTILE;
+  t->vj = JV;
   t->nt = tp.nt;
   t->vec = V;
   t->W = 1;
@@ -668,6 +671,7 @@ int choose_vtile(const HpttProblem &p, const TileParams &tp, HpttTile *t) {
   int nvy = 8;
   while (nvy * V - V + 1 < TY) nvy *= 2;
   const int R2 = R;
+  if (nvx / 8 > JV || nvy / 8 > JV) return ST_TOO_LARGE;
   if (cdiv(TY, R1) * (nvx / 8) > JV || cdiv(TX, R2) * (nvy / 8) > JV) return ST_TOO_LARGE;
   t->vlx = log2_slots(nvx);
   t->vly = log2_slots(nvy);
@@ -1046,7 +1050,8 @@ std::string describe(const HpttProblem &p, const HpttTile &t) {
      << ", " << t.nt << " threads/CTA";
   if (t.kind == KIND_ROWS) os << ", vector " << t.vec;
   if (t.kind == KIND_VTILE)
-    os << ", slots " << (8 << t.vlx) << " x " << (8 << t.vly) << ", J " << t.J1 << "/" << t.J2;
+    os << ", slots " << (8 << t.vlx) << " x " << (8 << t.vly) << ", J " << t.J1 << "/" << t.J2
+       << ", " << t.vj << " vectors/thread";
   os << "\n  tile W=" << t.W << " X{";
   for (int i = 0; i < t.nx; ++i) os << (i ? "," : "") << t.xd[i] << ":" << t.xt[i];
   os << "} Y{";

@@ -61,6 +61,8 @@ struct TileParams {
                            // allows one, else the tile above
   int vt_nvx = 16;         // vector slots along a row (load) and along a
   int vt_nvy = 16;         // column (store) of a vector tile: 8, 16 or 32
+  int vt_j = 8;            // 16-byte vectors a vector-tile thread holds per
+                           // phase: 8 (64 registers) or 4 (32 registers)
 };
 
 // Whether a vector tile (KIND_VTILE) can serve this problem: elements of at

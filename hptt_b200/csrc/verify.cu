@@ -326,7 +326,8 @@ int replay_vtile(const HpttProblem &P, const HpttTile &T, int update, const Layo
                  uint64_t *checked, int misA, int misB) {
   const int esz = elem_bytes(P.dtype);
   const int V = 16 / esz, PD = V - 1;
-  const int JV = hptt_vt_jmax();
+  const int JV = T.vj;
+  if (JV != 4 && JV != 8) return 300;
   if (V < 2) return 301;
   const int nvx = 8 << T.vlx, nvy = 8 << T.vly;
   const int GX = nvx / 8, GY = nvy / 8;  // slots of a line a thread takes
@@ -603,8 +604,8 @@ extern "C" int hptt_cuda_debug_check_indexing(int dtype, uint32_t rank, const ui
   // with the B-window checks covers both settings.
   if (vtile_possible(P)) {
     const int V = 16 / elem_bytes(P.dtype);
-    const int shapes[][4] = {{256, 16, 16, 0}, {256, 16, 32, 1}, {512, 32, 32, 0},
-                             {256, 32, 8, 1},  {512, 8, 32, 0}};
+    const int shapes[][5] = {{256, 16, 16, 0, 8}, {256, 16, 32, 1, 4}, {512, 32, 32, 0, 8},
+                             {256, 32, 8, 1, 8},  {512, 8, 32, 0, 4}};
     for (const auto &sh : shapes) {
       {
         const int update = 1;
@@ -614,6 +615,7 @@ extern "C" int hptt_cuda_debug_check_indexing(int dtype, uint32_t rank, const ui
         vp.vt_nvx = sh[1];
         vp.vt_nvy = sh[2];
         vp.grid_order = sh[3];
+        vp.vt_j = sh[4];
         HpttTile T;
         st = choose_tile(P, vp, update, &T);
         if (st != ST_OK) return st;
@@ -635,8 +637,8 @@ extern "C" int hptt_cuda_debug_check_indexing(int dtype, uint32_t rank, const ui
 extern "C" int hptt_cuda_debug_check_vtile(int dtype, uint32_t rank, const uint32_t *in_size,
                                            const uint32_t *perm, const uint32_t *in_outer,
                                            const uint32_t *out_outer, int nt, int nvx, int nvy,
-                                           int grid_order, int update, int mis_a, int mis_b,
-                                           uint64_t *checked) {
+                                           int vj, int grid_order, int update, int mis_a,
+                                           int mis_b, uint64_t *checked) {
   HpttProblem P;
   Layout L;
   std::vector<uint8_t> inner;
@@ -648,6 +650,7 @@ extern "C" int hptt_cuda_debug_check_vtile(int dtype, uint32_t rank, const uint3
   vp.nt = nt;
   vp.vt_nvx = nvx;
   vp.vt_nvy = nvy;
+  vp.vt_j = vj;
   vp.grid_order = grid_order;
   HpttTile T;
   st = choose_tile(P, vp, update, &T);

@@ -50,7 +50,7 @@
 namespace hptt_b200 {
 namespace dev {
 
-// Vector loads (rows) or stores (columns) a thread keeps in flight per phase.
+// The most 16-byte vectors a thread holds per phase (HpttTile::vj is 4 or 8).
 HPTT_HD constexpr int hptt_vt_jmax() { return 8; }
 
 // Thread `tid` -> (first window slot k of its lines, first line r0) of
@@ -103,7 +103,7 @@ __device__ __forceinline__ int vt_shift(const E *p) {
 // window shift is (shift of the tile origin + row offset) mod V.  Every
 // window of a row below limY goes to shared memory whole: a window that was
 // not read (it starts at or past limX) lands in the row's padding.
-template <typename E, typename OffT, bool LY, int LG>
+template <typename E, typename OffT, bool LY, int LG, int JV>
 __device__ __forceinline__ void vt_load(const HpttTile &T, const E *__restrict__ a0,
                                         const OffT *__restrict__ tabY, E *sm, int limX,
                                         int limY) {
@@ -115,7 +115,7 @@ __device__ __forceinline__ void vt_load(const HpttTile &T, const E *__restrict__
   const int R1 = T.R1;
   const int s0 = vt_shift(a0);
   const int LD = T.LD;
-  with_trip_count<hptt_vt_jmax() / G>(T.J1, [&](auto nn) {
+  with_trip_count<JV / G>(T.J1, [&](auto nn) {
     constexpr int N = decltype(nn)::value;
     VecT v[N][G];
     int sh[N];
@@ -150,7 +150,7 @@ __device__ __forceinline__ void vt_load(const HpttTile &T, const E *__restrict__
 // slots k + 8 g of columns c0 + j * R2; slot element i is y = V (k + 8 g) - t
 // + i, t the column's window shift.  When B is read, all of the thread's B
 // windows are read first.
-template <typename E, int MODE, bool UPD, typename OffT, bool LX, int LG>
+template <typename E, int MODE, bool UPD, typename OffT, bool LX, int LG, int JV>
 __device__ __forceinline__ void vt_store(const HpttTile &T, E *__restrict__ b0,
                                          const OffT *__restrict__ tabX, const E *sm,
                                          const Op<E, MODE, UPD> &op, int limX, int limY) {
@@ -162,7 +162,7 @@ __device__ __forceinline__ void vt_store(const HpttTile &T, E *__restrict__ b0,
   const int R2 = T.R2;
   const int t0 = vt_shift(b0);
   const int LD = T.LD;
-  with_trip_count<hptt_vt_jmax() / G>(T.J2, [&](auto nn) {
+  with_trip_count<JV / G>(T.J2, [&](auto nn) {
     constexpr int N = decltype(nn)::value;
     // column j's offset and window shift (-1: outside the tile)
     auto column = [&](int j, OffT &off) -> int {
@@ -223,7 +223,7 @@ __device__ __forceinline__ void vt_store(const HpttTile &T, E *__restrict__ b0,
   });
 }
 
-template <typename E, int MODE, bool UPD, typename OffT, bool LX, bool LY>
+template <typename E, int MODE, bool UPD, typename OffT, bool LX, bool LY, int JV>
 __device__ __forceinline__ void vtile_one(const HpttProblem &P, const HpttTile &T,
                                           const E *__restrict__ A, E *__restrict__ B,
                                           const unsigned char *__restrict__ tables,
@@ -237,20 +237,21 @@ __device__ __forceinline__ void vtile_one(const HpttProblem &P, const HpttTile &
   const OffT *__restrict__ tabY = reinterpret_cast<const OffT *>(tables);
   const OffT *__restrict__ tabX = reinterpret_cast<const OffT *>(tables + T.tab2_off);
   const E *a0 = A + o.bA;
+  static_assert(JV == 4 || JV == 8, "4 or 8 vectors per thread");
   if (T.vlx == 0)
-    vt_load<E, OffT, LY, 0>(T, a0, tabY, sm, limX, limY);
+    vt_load<E, OffT, LY, 0, JV>(T, a0, tabY, sm, limX, limY);
   else if (T.vlx == 1)
-    vt_load<E, OffT, LY, 1>(T, a0, tabY, sm, limX, limY);
+    vt_load<E, OffT, LY, 1, JV>(T, a0, tabY, sm, limX, limY);
   else
-    vt_load<E, OffT, LY, 2>(T, a0, tabY, sm, limX, limY);
+    vt_load<E, OffT, LY, 2, JV>(T, a0, tabY, sm, limX, limY);
   __syncthreads();
   E *b0 = B + o.bB;
   if (T.vly == 0)
-    vt_store<E, MODE, UPD, OffT, LX, 0>(T, b0, tabX, sm, op, limX, limY);
+    vt_store<E, MODE, UPD, OffT, LX, 0, JV>(T, b0, tabX, sm, op, limX, limY);
   else if (T.vly == 1)
-    vt_store<E, MODE, UPD, OffT, LX, 1>(T, b0, tabX, sm, op, limX, limY);
+    vt_store<E, MODE, UPD, OffT, LX, 1, JV>(T, b0, tabX, sm, op, limX, limY);
   else
-    vt_store<E, MODE, UPD, OffT, LX, 2>(T, b0, tabX, sm, op, limX, limY);
+    vt_store<E, MODE, UPD, OffT, LX, 2, JV>(T, b0, tabX, sm, op, limX, limY);
 }
 
 }  // namespace dev

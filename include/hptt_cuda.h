@@ -164,8 +164,9 @@ int hptt_cuda_debug_check_indexing(int dtype, uint32_t rank, const uint32_t *in_
                                    uint64_t *checked);
 
 /* The same replay for one vector-tile form: threads per CTA `nt`, window
- * slots per row `nvx` and per column `nvy` (8, 16 or 32), grid order
- * `grid_order`, whether B is read (`update`), and the A and B base addresses
+ * slots per row `nvx` and per column `nvy` (8, 16 or 32), 16-byte vectors per
+ * thread and phase `vj` (4 or 8), grid order `grid_order`, whether B is read
+ * (`update`), and the A and B base addresses
  * `mis_a` / `mis_b` elements past a 16-byte boundary.  Returns 0 when the
  * checks hold (also when the problem takes no vector tile: *checked is then
  * 0), else a diagnostic code >= 2000.  Extension, for tests; no reference
@@ -173,7 +174,7 @@ int hptt_cuda_debug_check_indexing(int dtype, uint32_t rank, const uint32_t *in_
 int hptt_cuda_debug_check_vtile(int dtype, uint32_t rank, const uint32_t *in_size,
                                 const uint32_t *perm, const uint32_t *in_outer,
                                 const uint32_t *out_outer, int nt, int nvx, int nvy,
-                                int grid_order, int update, int mis_a, int mis_b,
+                                int vj, int grid_order, int update, int mis_a, int mis_b,
                                 uint64_t *checked);
 
 /* Size of the fixed device array hptt_cuda_transpose_noalloc keeps its

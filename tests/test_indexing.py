@@ -124,16 +124,16 @@ def test_replay_random_ranks_7_and_8(seed):
     assert n == np.prod(size)
 
 
-def check_vtile(dtype, size, perm, nt, nvx, nvy, order, update, mis_a, mis_b):
+def check_vtile(dtype, size, perm, nt, nvx, nvy, order, update, mis_a, mis_b, vj=8):
     lib = h.load_library()
     f = lib.hptt_cuda_debug_check_vtile
     f.argtypes = [ctypes.c_int, ctypes.c_uint32, _u32p, _u32p, _u32p, _u32p] + \
-        [ctypes.c_int] * 7 + [ctypes.POINTER(ctypes.c_uint64)]
+        [ctypes.c_int] * 8 + [ctypes.POINTER(ctypes.c_uint64)]
     f.restype = ctypes.c_int
     u = lambda v: (ctypes.c_uint32 * len(v))(*v)  # noqa: E731
     n = ctypes.c_uint64(0)
-    rc = f(h.dtype_code(dtype), len(size), u(size), u(perm), None, None, nt, nvx, nvy, order,
-           update, mis_a, mis_b, ctypes.byref(n))
+    rc = f(h.dtype_code(dtype), len(size), u(size), u(perm), None, None, nt, nvx, nvy, vj,
+           order, update, mis_a, mis_b, ctypes.byref(n))
     return rc, n.value
 
 
@@ -157,18 +157,20 @@ VTILE_SHAPES = [
 
 @pytest.mark.parametrize("dt,size,perm", VTILE_SHAPES)
 def test_replay_vtile_every_tuner_form(dt, size, perm):
-    """Every window-slot shape, thread count and grid order the autotuner
-    times, with both update settings and base addresses on and off a 16-byte
-    boundary."""
+    """Every window-slot shape, thread count, vectors per thread and grid
+    order the autotuner times, with both update settings and base addresses
+    on and off a 16-byte boundary."""
     v = 16 // {"f32": 4, "f64": 8, "c64": 8}[dt]
     used = 0
-    for nt in (256, 512):
-        for nvx in (8, 16, 32):
-            for nvy in (8, 16, 32):
-                for order in (0, 1):
-                    for update, ma, mb in ((0, 0, 0), (1, v - 1, 1)):
-                        rc, n = check_vtile(dt, size, perm, nt, nvx, nvy, order, update, ma, mb)
-                        assert rc == 0, (dt, size, perm, nt, nvx, nvy, order, update, ma, mb, rc)
+    for vj in (8, 4):
+        for nt in (256, 512):
+            for nvx in (8, 16, 32):
+                for nvy in (8, 16, 32):
+                    for k, (update, ma, mb) in enumerate(((0, 0, 0), (1, v - 1, 1))):
+                        order = k ^ (nvx == 16)
+                        rc, n = check_vtile(dt, size, perm, nt, nvx, nvy, order, update, ma, mb,
+                                            vj)
+                        assert rc == 0, (dt, size, perm, nt, nvx, nvy, vj, order, update, rc)
                         assert n in (0, np.prod(size))
                         used += n > 0
     assert used > 0, "no vector tile planned"
