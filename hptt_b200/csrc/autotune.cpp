@@ -39,7 +39,7 @@ const char *env_path() { return std::getenv("HPTT_B200_TUNE_CACHE"); }
 
 // Cache file: one line per key,
 // "key|run vmin smem rows_min y_first iters full_side walk upd_exact nt
-//  grid_order vt vt_nvx vt_nvy vt_j"
+//  grid_order vt vt_nvx vt_nvy vt_j vt_pre"
 // (missing trailing fields read as 0, walk and upd_exact as 1, nt as 256,
 // vt_nvx and vt_nvy as 16, vt_j as 8).
 void read_cache_stream(std::istream &f) {
@@ -61,6 +61,7 @@ void read_cache_stream(std::istream &f) {
       if (!(v >> tp.vt_nvx)) tp.vt_nvx = 16;
       if (!(v >> tp.vt_nvy)) tp.vt_nvy = 16;
       if (!(v >> tp.vt_j) || (tp.vt_j != 4 && tp.vt_j != 8)) tp.vt_j = 8;
+      if (!(v >> tp.vt_pre)) tp.vt_pre = 0;
       g_cache[line.substr(0, bar)] = tp;
     }
   }
@@ -84,7 +85,7 @@ int write_cache(const char *path) {
       << kv.second.y_first << " " << kv.second.max_iters << " " << kv.second.full_side << " "
       << kv.second.walk << " " << kv.second.upd_exact << " " << kv.second.nt << " "
       << kv.second.grid_order << " " << kv.second.vt << " " << kv.second.vt_nvx << " "
-      << kv.second.vt_nvy << " " << kv.second.vt_j << "\n";
+      << kv.second.vt_nvy << " " << kv.second.vt_j << " " << kv.second.vt_pre << "\n";
   return ST_OK;
 }
 
@@ -93,7 +94,7 @@ int write_cache(const char *path) {
 // (the kernel's limit or half of it: smaller tiles, more CTAs), and whether a
 // single-dim side takes its whole extent.  Candidates that plan the same tile
 // as an earlier one are not timed again.
-std::vector<TileParams> candidates(const HpttProblem &prob) {
+std::vector<TileParams> candidates(const HpttProblem &prob, int update) {
   const int elem_size = elem_bytes(prob.dtype);
   std::vector<TileParams> c;
   // vector tiles first (window slots per row and per column, threads per
@@ -112,6 +113,11 @@ std::vector<TileParams> candidates(const HpttProblem &prob) {
               tp.vt_nvy = nvy;
               tp.grid_order = go;
               c.push_back(tp);
+              // update tiles: the four-vector build with B read first
+              if (update && vj == 4 && go == 0) {
+                tp.vt_pre = 1;
+                c.push_back(tp);
+              }
             }
   for (int full : {0, 1, 2})
     for (int iters : {0, hptt_jmax_tile(elem_size) / 2})
@@ -199,7 +205,7 @@ int autotune(Plan *p, double timeout, TileParams *best) {
   void *user_B = p->args.B;
   p->args.B = scratch;
   std::vector<HpttTile> timed;  // tiles already timed (identical plans skip)
-  std::vector<TileParams> cands = candidates(p->args.p);
+  std::vector<TileParams> cands = candidates(p->args.p, p->args.update);
   struct Timing {
     float ms;
     TileParams tp;

@@ -139,8 +139,9 @@ struct HpttTile {
   // (vlx) and along a column of the store phase (vly); a row has 8 << vlx
   // vector slots, a column 8 << vly; vj = the most 16-byte vectors a thread
   // holds per phase (4 or 8: two kernel builds with their own register
-  // budgets)
-  int32_t vlx, vly, vj;
+  // budgets); vpre = 1: an update tile of the four-vector build reads its B
+  // windows before its A loads
+  int32_t vlx, vly, vj, vpre;
 };
 
 // One slot of a KIND_TILE offset table (OffT = uint32_t or int64_t).

@@ -590,7 +590,7 @@ int log2_slots(int n) { return n >= 32 ? 2 : (n >= 16 ? 1 : 0); }
 // Each side takes whole dims while its run fits the window slots
 // (nvx * V - V + 1 elements: any start shift fits) and the per-thread
 // iterations, then a balanced chunk of the next dim.
-int choose_vtile(const HpttProblem &p, const TileParams &tp, HpttTile *t) {
+int choose_vtile(const HpttProblem &p, const TileParams &tp, int update, HpttTile *t) {
   const int sz = elem_bytes(p.dtype);
   if (!vtile_possible(p)) return ST_TOO_LARGE;
   const int V = 16 / sz;
@@ -600,6 +600,7 @@ int choose_vtile(const HpttProblem &p, const TileParams &tp, HpttTile *t) {
   std::memset(t, 0, sizeof(*t));
   t->kind = KIND_VTILE;
   t->vj = JV;
+  t->vpre = (tp.vt_pre && update && JV == 4) ? 1 : 0;
   t->nt = tp.nt;
   t->vec = V;
   t->W = 1;
@@ -746,14 +747,15 @@ void vtile_maps(const HpttProblem &p, const HpttTile &t, std::vector<int64_t> *r
 }
 
 int choose_tile(const HpttProblem &p, const TileParams &tp, int update, HpttTile *t) {
-  (void)update;  // the shapes are the same with and without the B read
+  // the shapes are the same with and without the B read (only the vector
+  // tile's early B reads depend on it)
   const int sz = elem_bytes(p.dtype);
   const int r = p.rank;
   const bool common = p.perm[0] == 0;
   if (r == 1 || (common && p.n[0] * sz >= tp.rows_min_bytes))
     return choose_rows(p, tp, t);
   if (common && p.n[0] > tp.nt / 2) return choose_rows(p, tp, t);
-  if (tp.vt && vtile_possible(p) && choose_vtile(p, tp, t) == ST_OK) return ST_OK;
+  if (tp.vt && vtile_possible(p) && choose_vtile(p, tp, update, t) == ST_OK) return ST_OK;
 
   std::memset(t, 0, sizeof(*t));
   t->kind = KIND_TILE;
@@ -1051,7 +1053,7 @@ std::string describe(const HpttProblem &p, const HpttTile &t) {
   if (t.kind == KIND_ROWS) os << ", vector " << t.vec;
   if (t.kind == KIND_VTILE)
     os << ", slots " << (8 << t.vlx) << " x " << (8 << t.vly) << ", J " << t.J1 << "/" << t.J2
-       << ", " << t.vj << " vectors/thread";
+       << ", " << t.vj << " vectors/thread" << (t.vpre ? ", B read first" : "");
   os << "\n  tile W=" << t.W << " X{";
   for (int i = 0; i < t.nx; ++i) os << (i ? "," : "") << t.xd[i] << ":" << t.xt[i];
   os << "} Y{";

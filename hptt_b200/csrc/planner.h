@@ -63,6 +63,8 @@ struct TileParams {
   int vt_nvy = 16;         // column (store) of a vector tile: 8, 16 or 32
   int vt_j = 8;            // 16-byte vectors a vector-tile thread holds per
                            // phase: 8 (64 registers) or 4 (32 registers)
+  int vt_pre = 0;          // 1: update tiles with vt_j == 4 read B before A
+                           // (64 registers)
 };
 
 // Whether a vector tile (KIND_VTILE) can serve this problem: elements of at

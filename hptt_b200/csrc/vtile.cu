@@ -16,8 +16,10 @@ namespace {
 // registers (2048; a few variants spill up to 12 bytes).  Measured per shape,
 // neither wins everywhere: the f32 2D update {35014, 1428} ran 6.1 TB/s with
 // four and 6.0 with eight, the rank-6 {30, 4, 34, 42, 29, 10} copy 5.0 and 5.1.
-template <typename E, int MODE, bool UPD, typename OffT, bool LX, bool LY, int JV>
-__global__ void __launch_bounds__(512, JV == 8 ? 2 : 4)
+// Update tiles of the four-vector build can also read their B windows before
+// the A loads (PRE, HpttTile::vpre), with the eight-vector build's budget.
+template <typename E, int MODE, bool UPD, typename OffT, bool LX, bool LY, int JV, bool PRE>
+__global__ void __launch_bounds__(512, (JV == 8 || PRE) ? 2 : 4)
     k_vtile(const __grid_constant__ HpttArgs args) {
   // programmatic dependent launch: as in k_tile (kernels.cu)
   asm volatile("griddepcontrol.wait;\n" ::: "memory");
@@ -25,7 +27,7 @@ __global__ void __launch_bounds__(512, JV == 8 ? 2 : 4)
   extern __shared__ __align__(16) unsigned char smem[];
   const Scal sc{args.alpha[0], args.alpha[1], args.beta[0], args.beta[1]};
   const Op<E, MODE, UPD> op(sc);
-  vtile_one<E, MODE, UPD, OffT, LX, LY, JV>(args.p, args.t, static_cast<const E *>(args.A),
+  vtile_one<E, MODE, UPD, OffT, LX, LY, JV, PRE>(args.p, args.t, static_cast<const E *>(args.A),
                                             static_cast<E *>(args.B),
                                             static_cast<const unsigned char *>(args.tables), op,
                                             reinterpret_cast<E *>(smem), blockIdx.x);
@@ -33,21 +35,28 @@ __global__ void __launch_bounds__(512, JV == 8 ? 2 : 4)
 
 // 64-bit offsets read both sides from the tables; 32-bit offsets compute a
 // single-dim side as q * stride.
-template <typename E, int MODE, bool UPD, int JV>
+template <typename E, int MODE, bool UPD, int JV, bool PRE>
 const void *pick_side(const HpttTile &t) {
   if (t.big_offsets)
-    return reinterpret_cast<const void *>(&k_vtile<E, MODE, UPD, int64_t, false, false, JV>);
+    return reinterpret_cast<const void *>(&k_vtile<E, MODE, UPD, int64_t, false, false, JV, PRE>);
   const bool lx = t.nx <= 1, ly = t.ny <= 1;
   if (lx && ly)
-    return reinterpret_cast<const void *>(&k_vtile<E, MODE, UPD, uint32_t, true, true, JV>);
-  if (lx) return reinterpret_cast<const void *>(&k_vtile<E, MODE, UPD, uint32_t, true, false, JV>);
-  if (ly) return reinterpret_cast<const void *>(&k_vtile<E, MODE, UPD, uint32_t, false, true, JV>);
-  return reinterpret_cast<const void *>(&k_vtile<E, MODE, UPD, uint32_t, false, false, JV>);
+    return reinterpret_cast<const void *>(&k_vtile<E, MODE, UPD, uint32_t, true, true, JV, PRE>);
+  if (lx)
+    return reinterpret_cast<const void *>(&k_vtile<E, MODE, UPD, uint32_t, true, false, JV, PRE>);
+  if (ly)
+    return reinterpret_cast<const void *>(&k_vtile<E, MODE, UPD, uint32_t, false, true, JV, PRE>);
+  return reinterpret_cast<const void *>(&k_vtile<E, MODE, UPD, uint32_t, false, false, JV, PRE>);
 }
 
 template <typename E, int MODE, bool UPD>
 const void *pick_shape(const HpttTile &t) {
-  return t.vj == 4 ? pick_side<E, MODE, UPD, 4>(t) : pick_side<E, MODE, UPD, 8>(t);
+  if (t.vj == 4) {
+    if constexpr (UPD)
+      if (t.vpre) return pick_side<E, MODE, UPD, 4, true>(t);
+    return pick_side<E, MODE, UPD, 4, false>(t);
+  }
+  return pick_side<E, MODE, UPD, 8, false>(t);
 }
 
 }  // namespace

@@ -150,10 +150,48 @@ __device__ __forceinline__ void vt_load(const HpttTile &T, const E *__restrict__
 // slots k + 8 g of columns c0 + j * R2; slot element i is y = V (k + 8 g) - t
 // + i, t the column's window shift.  When B is read, all of the thread's B
 // windows are read first.
-template <typename E, int MODE, bool UPD, typename OffT, bool LX, int LG, int JV>
+// Column j's B offset and window shift, -1 when the column is outside the
+// tile (shared by the store phase and the early B reads).
+template <typename E, typename OffT, bool LX>
+__device__ __forceinline__ int vt_column(const HpttTile &T, const OffT *__restrict__ tabX,
+                                         int x, int t0, int limX, OffT &off) {
+  constexpr int V = 16 / sizeof(E);
+  off = LX ? static_cast<OffT>(x) * static_cast<OffT>(T.sxb) : tabX[min(x, T.TX - 1)];
+  const int t = (t0 + static_cast<int>(off)) & (V - 1);
+  return x < limX ? t : -1;
+}
+
+// The store phase's B windows, read before the load phase so they are in
+// flight together with the A loads (update tiles, HpttTile::vpre): slot g of
+// the thread's column j lands in bv[j * G + g].
+template <typename E, typename OffT, bool LX, int LG, int JV>
+__device__ __forceinline__ void vt_bread(const HpttTile &T, const E *__restrict__ b0,
+                                         const OffT *__restrict__ tabX,
+                                         Vec<E, 16 / sizeof(E)> *bv, int limX, int limY) {
+  constexpr int V = 16 / sizeof(E);
+  constexpr int G = 1 << LG;
+  const VtPos ps = vt_pos(threadIdx.x);
+  const int yk = ps.k * V;
+  const int t0 = vt_shift(b0);
+  with_trip_count<JV / G>(T.J2, [&](auto nn) {
+    constexpr int N = decltype(nn)::value;
+#pragma unroll
+    for (int j = 0; j < N; ++j) {
+      OffT off;
+      const int t = vt_column<E, OffT, LX>(T, tabX, ps.r0 + j * T.R2, t0, limX, off);
+      const E *w = b0 + static_cast<int64_t>(off) + (yk - t);
+#pragma unroll
+      for (int g = 0; g < G; ++g)
+        if (t >= 0 && yk + 8 * V * g - t < limY) bv[j * G + g] = ld_vec_rw<E, V>(w + 8 * V * g);
+    }
+  });
+}
+
+template <typename E, int MODE, bool UPD, typename OffT, bool LX, int LG, int JV, bool PRE>
 __device__ __forceinline__ void vt_store(const HpttTile &T, E *__restrict__ b0,
                                          const OffT *__restrict__ tabX, const E *sm,
-                                         const Op<E, MODE, UPD> &op, int limX, int limY) {
+                                         const Op<E, MODE, UPD> &op, int limX, int limY,
+                                         const Vec<E, 16 / sizeof(E)> *pre) {
   constexpr int V = 16 / sizeof(E);
   constexpr int G = 1 << LG;
   using VecT = Vec<E, V>;
@@ -166,13 +204,10 @@ __device__ __forceinline__ void vt_store(const HpttTile &T, E *__restrict__ b0,
     constexpr int N = decltype(nn)::value;
     // column j's offset and window shift (-1: outside the tile)
     auto column = [&](int j, OffT &off) -> int {
-      const int x = ps.r0 + j * R2;
-      off = LX ? static_cast<OffT>(x) * static_cast<OffT>(T.sxb) : tabX[min(x, T.TX - 1)];
-      const int t = (t0 + static_cast<int>(off)) & (V - 1);
-      return x < limX ? t : -1;
+      return vt_column<E, OffT, LX>(T, tabX, ps.r0 + j * R2, t0, limX, off);
     };
-    VecT bv[UPD ? N : 1][UPD ? G : 1];
-    if (UPD) {
+    VecT bv[UPD && !PRE ? N : 1][UPD && !PRE ? G : 1];
+    if (UPD && !PRE) {
 #pragma unroll
       for (int j = 0; j < N; ++j) {
         OffT off;
@@ -181,7 +216,7 @@ __device__ __forceinline__ void vt_store(const HpttTile &T, E *__restrict__ b0,
 #pragma unroll
         for (int g = 0; g < G; ++g)
           if (t >= 0 && yk + 8 * V * g - t < limY)
-            bv[UPD ? j : 0][UPD ? g : 0] = ld_vec_rw<E, V>(w + 8 * V * g);
+            bv[UPD && !PRE ? j : 0][UPD && !PRE ? g : 0] = ld_vec_rw<E, V>(w + 8 * V * g);
       }
     }
 #pragma unroll
@@ -199,7 +234,8 @@ __device__ __forceinline__ void vt_store(const HpttTile &T, E *__restrict__ b0,
 #pragma unroll
         for (int i = 0; i < V; ++i) {
           const E a = s[(8 * V * g + i) * LD];
-          r.v[i] = op(a, UPD ? bv[UPD ? j : 0][UPD ? g : 0].v[i] : a);
+          const E b = !UPD ? a : (PRE ? pre[j * G + g].v[i] : bv[PRE ? 0 : j][PRE ? 0 : g].v[i]);
+          r.v[i] = op(a, b);
         }
         E *dst = w + 8 * V * g;
         if (y0 >= 0 && y0 + V <= limY) {
@@ -223,7 +259,7 @@ __device__ __forceinline__ void vt_store(const HpttTile &T, E *__restrict__ b0,
   });
 }
 
-template <typename E, int MODE, bool UPD, typename OffT, bool LX, bool LY, int JV>
+template <typename E, int MODE, bool UPD, typename OffT, bool LX, bool LY, int JV, bool PRE>
 __device__ __forceinline__ void vtile_one(const HpttProblem &P, const HpttTile &T,
                                           const E *__restrict__ A, E *__restrict__ B,
                                           const unsigned char *__restrict__ tables,
@@ -238,6 +274,17 @@ __device__ __forceinline__ void vtile_one(const HpttProblem &P, const HpttTile &
   const OffT *__restrict__ tabX = reinterpret_cast<const OffT *>(tables + T.tab2_off);
   const E *a0 = A + o.bA;
   static_assert(JV == 4 || JV == 8, "4 or 8 vectors per thread");
+  static_assert(!PRE || UPD, "early B reads for update tiles only");
+  E *b0 = B + o.bB;
+  Vec<E, V> bpre[PRE ? JV : 1];
+  if (PRE) {
+    if (T.vly == 0)
+      vt_bread<E, OffT, LX, 0, JV>(T, b0, tabX, bpre, limX, limY);
+    else if (T.vly == 1)
+      vt_bread<E, OffT, LX, 1, JV>(T, b0, tabX, bpre, limX, limY);
+    else
+      vt_bread<E, OffT, LX, 2, JV>(T, b0, tabX, bpre, limX, limY);
+  }
   if (T.vlx == 0)
     vt_load<E, OffT, LY, 0, JV>(T, a0, tabY, sm, limX, limY);
   else if (T.vlx == 1)
@@ -245,13 +292,12 @@ __device__ __forceinline__ void vtile_one(const HpttProblem &P, const HpttTile &
   else
     vt_load<E, OffT, LY, 2, JV>(T, a0, tabY, sm, limX, limY);
   __syncthreads();
-  E *b0 = B + o.bB;
   if (T.vly == 0)
-    vt_store<E, MODE, UPD, OffT, LX, 0, JV>(T, b0, tabX, sm, op, limX, limY);
+    vt_store<E, MODE, UPD, OffT, LX, 0, JV, PRE>(T, b0, tabX, sm, op, limX, limY, bpre);
   else if (T.vly == 1)
-    vt_store<E, MODE, UPD, OffT, LX, 1, JV>(T, b0, tabX, sm, op, limX, limY);
+    vt_store<E, MODE, UPD, OffT, LX, 1, JV, PRE>(T, b0, tabX, sm, op, limX, limY, bpre);
   else
-    vt_store<E, MODE, UPD, OffT, LX, 2, JV>(T, b0, tabX, sm, op, limX, limY);
+    vt_store<E, MODE, UPD, OffT, LX, 2, JV, PRE>(T, b0, tabX, sm, op, limX, limY, bpre);
 }
 
 }  // namespace dev

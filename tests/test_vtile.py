@@ -29,9 +29,11 @@ SHAPES = [
     ("c64", [5, 3, 7, 40, 9], [3, 4, 0, 2, 1]),
 ]
 
-# (threads, window slots per row, per column, grid order, vectors per thread)
-FORMS = [(256, 16, 16, 0, 8), (256, 32, 8, 1, 8), (512, 32, 32, 0, 8), (256, 8, 32, 0, 4),
-         (512, 8, 8, 1, 4), (512, 16, 32, 0, 4)]
+# (threads, window slots per row, per column, grid order, vectors per thread,
+# B read before the A loads -- update tiles of the four-vector build only)
+FORMS = [(256, 16, 16, 0, 8, 0), (256, 32, 8, 1, 8, 0), (512, 32, 32, 0, 8, 0),
+         (256, 8, 32, 0, 4, 0), (512, 8, 8, 1, 4, 0), (512, 16, 32, 0, 4, 0),
+         (256, 16, 32, 0, 4, 1), (512, 32, 16, 1, 4, 1)]
 
 
 def _run(name, size, perm, al, be, a, b0, offset, cs=None):
@@ -65,14 +67,13 @@ def _cache_line(tmp_path, name, size, perm, al, be, cs):
     (line,) = path.read_text().splitlines()
     key, fields = line.split("|")
     f = fields.split()
-    assert len(f) == 15
+    assert len(f) == 16
     return path, key, f
 
 
-def _force(path, key, f, nt, nvx, nvy, order, vj=8):
+def _force(path, key, f, nt, nvx, nvy, order, vj=8, pre=0):
     g = list(f)
-    g[9], g[10], g[11], g[12], g[13], g[14] = (str(nt), str(order), "1", str(nvx), str(nvy),
-                                               str(vj))
+    g[9:16] = [str(nt), str(order), "1", str(nvx), str(nvy), str(vj), str(pre)]
     path.write_text(key + "|" + " ".join(g) + "\n")
     h.tune_cache_clear()
     h.tune_cache_load(str(path))
@@ -95,13 +96,13 @@ def test_vector_tile_forms(tmp_path, name, size, perm, si):
     want = oracle_run(name, size, perm, al, be, a, b0, complex_scalars=cs)
     try:
         path, key, f = _cache_line(tmp_path, name, size, perm, al, be, cs)
-        for nt, nvx, nvy, order, vj in FORMS:
-            _force(path, key, f, nt, nvx, nvy, order, vj)
+        for nt, nvx, nvy, order, vj, pre in FORMS:
+            _force(path, key, f, nt, nvx, nvy, order, vj, pre)
             for offset in (0, ESZ[name], 3 * ESZ[name]):
                 got, desc = _run(name, size, perm, al, be, a, b0, offset, cs)
                 assert "vector tile" in desc, desc
                 assert_same(got, want, name,
-                            f"{size} {perm} a={al} b={be} form={nt},{nvx},{nvy},{order},{vj} "
+                            f"{size} {perm} a={al} b={be} form={nt},{nvx},{nvy},{order},{vj},{pre} "
                             f"offset={offset}")
     finally:
         h.tune_cache_clear()
