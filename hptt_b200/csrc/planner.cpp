@@ -588,8 +588,9 @@ int log2_slots(int n) { return n >= 32 ? 2 : (n >= 16 ? 1 : 0); }
 // strides chain (one contiguous run of A), never the output's leading dim;
 // Y: output dims 0, 1, ... not in X whose B strides chain (one run of B).
 // Each side takes whole dims while its run fits the window slots
-// (nvx * V - V + 1 elements: any start shift fits) and the per-thread
-// iterations, then a balanced chunk of the next dim.
+// (nvx * V - V + 1 elements: any start shift fits) and the other phase's
+// per-thread vectors (nt / 8 lines per pass, each line's slots / 8 vectors
+// per line, at most vt_j in all), then a balanced chunk of the next dim.
 int choose_vtile(const HpttProblem &p, const TileParams &tp, int update, HpttTile *t) {
   const int sz = elem_bytes(p.dtype);
   if (!vtile_possible(p)) return ST_TOO_LARGE;

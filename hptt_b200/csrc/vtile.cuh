@@ -32,8 +32,9 @@
 // Thread mapping (vt_pos): a warp covers 8 consecutive window slots of 4
 // rows (load) or of 4 columns (store), so every global access of a warp is
 // four 128-byte runs; a thread walks every eighth slot of its rows or
-// columns.  The host picks the row pitch LD that minimises shared-memory
-// bank conflicts of exactly these accesses (vtile_bank_cost).
+// columns, at most JV (4 or 8, HpttTile::vj) vectors per phase.  The host
+// picks the row pitch LD that minimises shared-memory bank conflicts of
+// exactly these accesses (vtile_bank_cost).
 //
 // This replaces the reference's 256-bit in-register micro kernels
 // (src/arch/avx2/kernel_trans_avx2.cc:21-467) for shapes whose contiguous
@@ -49,9 +50,6 @@
 
 namespace hptt_b200 {
 namespace dev {
-
-// The most 16-byte vectors a thread holds per phase (HpttTile::vj is 4 or 8).
-HPTT_HD constexpr int hptt_vt_jmax() { return 8; }
 
 // Thread `tid` -> (first window slot k of its lines, first line r0) of
 // either phase: a warp holds 8 consecutive slots of 4 lines (4 * 128 bytes
@@ -82,7 +80,6 @@ HPTT_HD inline int vt_lim_y(const HpttTile &T, const TileOrigin &o) {
 
 // Shared memory: element (x, y) at (y + V - 1) * LD + (x + V - 1); rows and
 // columns run from -(V - 1) so the windows' outside elements land in padding.
-HPTT_HD constexpr int vt_pad(int esz) { return 16 / esz - 1; }
 
 template <typename E, int V>
 __device__ __forceinline__ void st_vec_cs(E *p, const Vec<E, V> &v) {
@@ -98,7 +95,8 @@ __device__ __forceinline__ int vt_shift(const E *p) {
 }
 
 // Load phase: rows of A into shared memory.  Thread (k, r0) reads window
-// slots k + 8 g (g < G = 8 slots groups of a row) of rows r0 + j * R1.  A
+// slots k + 8 g (g < G, the row's number of 8-slot groups) of rows
+// r0 + j * R1, at most JV vectors in all.  A
 // row's offset steps by R1 * sya (one Y dim) or comes from the table; its
 // window shift is (shift of the tile origin + row offset) mod V.  Every
 // window of a row below limY goes to shared memory whole: a window that was
@@ -146,11 +144,7 @@ __device__ __forceinline__ void vt_load(const HpttTile &T, const E *__restrict__
   });
 }
 
-// Store phase: columns of B from shared memory.  Thread (k, c0) writes window
-// slots k + 8 g of columns c0 + j * R2; slot element i is y = V (k + 8 g) - t
-// + i, t the column's window shift.  When B is read, all of the thread's B
-// windows are read first.
-// Column j's B offset and window shift, -1 when the column is outside the
+// Column x's B offset and window shift, -1 when the column is outside the
 // tile (shared by the store phase and the early B reads).
 template <typename E, typename OffT, bool LX>
 __device__ __forceinline__ int vt_column(const HpttTile &T, const OffT *__restrict__ tabX,
@@ -187,6 +181,11 @@ __device__ __forceinline__ void vt_bread(const HpttTile &T, const E *__restrict_
   });
 }
 
+// Store phase: columns of B from shared memory.  Thread (k, c0) writes window
+// slots k + 8 g of columns c0 + j * R2; slot element i is y = V (k + 8 g) - t
+// + i, t the column's window shift.  When B is read, all of the thread's B
+// windows are read before the first store: here (PRE off) or, with PRE,
+// before the load phase (vt_bread, passed in as `pre`).
 template <typename E, int MODE, bool UPD, typename OffT, bool LX, int LG, int JV, bool PRE>
 __device__ __forceinline__ void vt_store(const HpttTile &T, E *__restrict__ b0,
                                          const OffT *__restrict__ tabX, const E *sm,
