@@ -13,6 +13,7 @@
 #include <map>
 #include <mutex>
 #include <sstream>
+#include <utility>
 #include <vector>
 
 #include "launch.h"
@@ -39,9 +40,9 @@ const char *env_path() { return std::getenv("HPTT_B200_TUNE_CACHE"); }
 
 // Cache file: one line per key,
 // "key|run vmin smem rows_min y_first iters full_side walk upd_exact nt
-//  grid_order vt vt_nvx vt_nvy vt_j vt_pre"
+//  grid_order vt vt_nvx vt_nvy vt_j vt_pre tt tt_kx tt_ky"
 // (missing trailing fields read as 0, walk and upd_exact as 1, nt as 256,
-// vt_nvx and vt_nvy as 16, vt_j as 8).
+// vt_nvx and vt_nvy as 16, vt_j as 8, tt_kx and tt_ky as 2).
 void read_cache_stream(std::istream &f) {
   std::string line;
   while (std::getline(f, line)) {
@@ -62,6 +63,9 @@ void read_cache_stream(std::istream &f) {
       if (!(v >> tp.vt_nvy)) tp.vt_nvy = 16;
       if (!(v >> tp.vt_j) || (tp.vt_j != 4 && tp.vt_j != 8)) tp.vt_j = 8;
       if (!(v >> tp.vt_pre)) tp.vt_pre = 0;
+      if (!(v >> tp.tt)) tp.tt = 0;
+      if (!(v >> tp.tt_kx)) tp.tt_kx = 2;
+      if (!(v >> tp.tt_ky)) tp.tt_ky = 2;
       g_cache[line.substr(0, bar)] = tp;
     }
   }
@@ -85,7 +89,8 @@ int write_cache(const char *path) {
       << kv.second.y_first << " " << kv.second.max_iters << " " << kv.second.full_side << " "
       << kv.second.walk << " " << kv.second.upd_exact << " " << kv.second.nt << " "
       << kv.second.grid_order << " " << kv.second.vt << " " << kv.second.vt_nvx << " "
-      << kv.second.vt_nvy << " " << kv.second.vt_j << " " << kv.second.vt_pre << "\n";
+      << kv.second.vt_nvy << " " << kv.second.vt_j << " " << kv.second.vt_pre << " "
+      << kv.second.tt << " " << kv.second.tt_kx << " " << kv.second.tt_ky << "\n";
   return ST_OK;
 }
 
@@ -97,7 +102,39 @@ int write_cache(const char *path) {
 std::vector<TileParams> candidates(const HpttProblem &prob, int update) {
   const int elem_size = elem_bytes(prob.dtype);
   std::vector<TileParams> c;
-  // vector tiles first (window slots per row and per column, threads per
+  // TMA tiles (boxes per tile, grid order), where the strides allow tensor
+  // maps and the boxes are mostly inside the tensor: a box is 128 bytes
+  // along input dim 0 and along the output's leading dim, and below half
+  // full (extents short against the box, or just past a multiple of it) it
+  // moves twice the bytes it stores
+  auto fill = [&](int64_t n) {
+    const int64_t box = 128 / elem_size;
+    return static_cast<double>(n) / static_cast<double>((n + box - 1) / box * box);
+  };
+  // (one CTA per tile: every box count; persistent CTAs: the small tiles,
+  // which fit several CTAs per SM, with two and three stages)
+  if (ttile_possible(prob) && fill(prob.n[0]) * fill(prob.n[prob.perm[0]]) >= 0.5) {
+    for (const auto &k : {std::make_pair(1, 1), std::make_pair(2, 1), std::make_pair(1, 2),
+                          std::make_pair(2, 2), std::make_pair(4, 1), std::make_pair(1, 4),
+                          std::make_pair(4, 2), std::make_pair(2, 4)})
+      for (int go : {0, 1}) {
+        TileParams tp;
+        tp.tt = 1;
+        tp.tt_kx = k.first;
+        tp.tt_ky = k.second;
+        tp.grid_order = go;
+        c.push_back(tp);
+      }
+    for (const auto &k : {std::make_pair(1, 1), std::make_pair(2, 1), std::make_pair(1, 2)})
+      for (int stages : {2, 3}) {
+        TileParams tp;
+        tp.tt = stages;
+        tp.tt_kx = k.first;
+        tp.tt_ky = k.second;
+        c.push_back(tp);
+      }
+  }
+  // vector tiles (window slots per row and per column, threads per
   // CTA, vectors per thread, grid order), where the shape allows one
   if (vtile_possible(prob))
     for (int vj : {8, 4})

@@ -241,9 +241,9 @@ int batch_layout(const std::vector<BatchEntry> &entries, int sms, BatchLayout *L
       d.a.t = p->tile_scalar;
       d.a.tables = p->dtab_scalar;
     }
-    if (d.a.t.nt != kNT || d.a.t.kind == KIND_VTILE) {
-      // a 512-thread or vector-tile plan: its tile planned for the batch
-      // kernels' 256-thread tile form
+    if (d.a.t.nt != kNT || d.a.t.kind == KIND_VTILE || d.a.t.kind == KIND_TTILE) {
+      // a 512-thread, vector-tile or TMA-tile plan: its tile planned for the
+      // batch kernels' 256-thread tile form
       d.a.t = p->tile_batch;
       d.a.tables = p->dtab_batch;
       vec = 1;

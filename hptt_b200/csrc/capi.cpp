@@ -56,7 +56,14 @@ int plan_tiles(Plan *p, const TileParams &params) {
   int st = choose_tile(p->args.p, params, p->args.update, &p->args.t);
   if (st != ST_OK) return st;
   p->vec = p->args.t.kind == KIND_ROWS ? p->args.t.vec : 1;
-  if (p->args.t.kind == KIND_ROWS && p->vec > 1) {
+  if (p->args.t.kind == KIND_TTILE) {
+    // pointers off a 16-byte boundary (no tensor map) take the element tile
+    TileParams sp = params;
+    sp.tt = 0;
+    sp.vt = 0;
+    st = choose_tile(p->args.p, sp, p->args.update, &p->tile_scalar);
+    if (st != ST_OK) return st;
+  } else if (p->args.t.kind == KIND_ROWS && p->vec > 1) {
     // same problem without vector accesses, for pointers that are not
     // aligned to the planned vector
     TileParams sp = params;
@@ -82,17 +89,19 @@ int plan_tiles(Plan *p, const TileParams &params) {
   };
   st = upload(p->args.p, p->args.t, &p->dtab);
   if (st != ST_OK) return st;
-  if (p->args.t.kind == KIND_ROWS && p->vec > 1) {
+  if ((p->args.t.kind == KIND_ROWS && p->vec > 1) || p->args.t.kind == KIND_TTILE) {
     st = upload(p->args.p, p->tile_scalar, &p->dtab_scalar);
     if (st != ST_OK) return st;
   } else {
     p->dtab_scalar = p->dtab;
   }
-  if (p->args.t.nt != kBatchThreads || p->args.t.kind == KIND_VTILE) {
+  if (p->args.t.nt != kBatchThreads || p->args.t.kind == KIND_VTILE ||
+      p->args.t.kind == KIND_TTILE) {
     // the batch kernels run the 256-thread tile and rows forms only
     TileParams bp = params;
     bp.nt = kBatchThreads;
     bp.vt = 0;
+    bp.tt = 0;
     bp.max_vec_bytes = elem_bytes(p->args.p.dtype);  // rows: the scalar form
     st = choose_tile(p->args.p, bp, p->args.update, &p->tile_batch);
     if (st != ST_OK) return st;
@@ -137,6 +146,14 @@ int plan_enqueue_with(const Plan *p, const void *A, void *B, cudaStream_t stream
   if (vec > 1) {
     const uintptr_t vb = static_cast<uintptr_t>(vec) * elem_bytes(a.p.dtype);
     if (reinterpret_cast<uintptr_t>(A) % vb || reinterpret_cast<uintptr_t>(B) % vb) vec = 1;
+  }
+  if (a.t.kind == KIND_TTILE &&
+      ((reinterpret_cast<uintptr_t>(A) | reinterpret_cast<uintptr_t>(B)) & 15)) {
+    // no tensor map for this base: the plan's element tile
+    a.t = p->tile_scalar;
+    a.tables = p->dtab_scalar;
+    const cudaError_t e2 = launch_single(a, 1, p->grid_scalar, stream);
+    return e2 == cudaSuccess ? ST_OK : ST_CUDA;
   }
   cudaError_t e;
   if (vec == p->vec) {

@@ -27,7 +27,10 @@ enum HpttMode : int32_t { MODE_COPY = 0, MODE_REAL = 1, MODE_CPLX = 2 };
 //   KIND_VTILE tiles whose X side is one contiguous run of A and whose Y side
 //              is one contiguous run of B, moved as 16-byte vectors (see
 //              vtile.cuh); elements of at most 8 bytes.
-enum HpttKind : int32_t { KIND_TILE = 0, KIND_ROWS = 1, KIND_VTILE = 2 };
+//   KIND_TTILE tiles of boxes loaded and stored by the tensor memory
+//              accelerator (see ttile.cuh); fused rank <= 5, 4- or 8-byte
+//              elements, strides other than the unit one multiples of 16 bytes.
+enum HpttKind : int32_t { KIND_TILE = 0, KIND_ROWS = 1, KIND_VTILE = 2, KIND_TTILE = 3 };
 
 // Fused problem.  Dimensions are listed in INPUT order; sA/sB are the strides
 // (in elements) of input dim d in A and in B.  perm[k] = input dim that is
@@ -142,6 +145,10 @@ struct HpttTile {
   // budgets); vpre = 1: an update tile of the four-vector build reads its B
   // windows before its A loads
   int32_t vlx, vly, vj, vpre;
+  // KIND_TTILE: boxes per tile along input dim 0 (tkx) and along the output's
+  // leading dim (tky); ts = 0: one CTA per tile, 2-4: persistent CTAs that
+  // keep ts tiles of loads in flight (a ring of ts stages)
+  int32_t tkx, tky, ts;
 };
 
 // One slot of a KIND_TILE offset table (OffT = uint32_t or int64_t).

@@ -110,6 +110,7 @@ const void *pick_mode_cplx(int mode, bool upd, const HpttTile &t, int vec) {
 
 const void *kernel_for(const HpttArgs &a, int vec) {
   if (a.t.kind == KIND_VTILE) return vtile_kernel_for(a);
+  if (a.t.kind == KIND_TTILE) return ttile_kernel_for(a);
   const bool upd = a.update != 0;
   switch (a.p.dtype) {
     case DT_F32: return pick_mode<float, unsigned int>(a.mode, upd, a.t, vec);
@@ -123,6 +124,7 @@ const void *kernel_for(const HpttArgs &a, int vec) {
 int kernel_threads() { return kMaxNT; }
 
 cudaError_t launch_single(const HpttArgs &a, int vec, int grid, cudaStream_t stream) {
+  if (a.t.kind == KIND_TTILE) return launch_ttile(a, grid, stream);
   (void)grid;  // one CTA per tile
   const void *fn = kernel_for(a, vec);
   if (!fn) return cudaErrorInvalidValue;

@@ -14,10 +14,20 @@ const void *kernel_for(const HpttArgs &a, int vec);
 // The vector-tile kernel (KIND_VTILE) for these arguments, or null.
 const void *vtile_kernel_for(const HpttArgs &a);
 
+// The TMA-tile kernel (KIND_TTILE) for these arguments, or null.
+const void *ttile_kernel_for(const HpttArgs &a);
+
+// Enqueue one KIND_TTILE transpose: encodes the tensor maps of A and B
+// (16-byte aligned bases required: cudaErrorMisalignedAddress otherwise) and
+// launches with them, one CTA per tile or (persistent form, HpttTile::ts)
+// min(grid, tiles) CTAs.
+cudaError_t launch_ttile(const HpttArgs &a, int grid, cudaStream_t stream);
+
 // Most threads per CTA the single-transpose kernels are compiled for.
 int kernel_threads();
 
-// Enqueue one transpose.  `grid` CTAs loop over the tiles.
+// Enqueue one transpose: one CTA per tile, except the persistent TMA tile,
+// whose `grid` CTAs loop over the tiles.
 cudaError_t launch_single(const HpttArgs &a, int vec, int grid, cudaStream_t stream);
 
 // Resident CTAs per SM for this launch shape (also raises the dynamic

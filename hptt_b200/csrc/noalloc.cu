@@ -111,6 +111,14 @@ extern "C" int hptt_cuda_transpose_noalloc(int dtype, uint32_t rank, const uint3
       vec = 1;
     }
   }
+  if (a.t.kind == KIND_TTILE &&
+      ((reinterpret_cast<uintptr_t>(in) | reinterpret_cast<uintptr_t>(out)) & 15)) {
+    // no tensor map for these bases: the element tile
+    tp.tt = 0;
+    tp.vt = 0;
+    st = choose_tile(a.p, tp, a.update, &a.t);
+    if (st != ST_OK) return st;
+  }
   if (a.t.num_tiles == 0) return HPTT_OK;
   if (a.t.table_bytes > HPTT_NOALLOC_TABLE_BYTES) return HPTT_ERR_TOO_LARGE;
 
@@ -130,9 +138,13 @@ extern "C" int hptt_cuda_transpose_noalloc(int dtype, uint32_t rank, const uint3
       cudaSuccess)
     return HPTT_ERR_CUDA;
   a.tables = tables;
-  int per_sm = 0;
-  if (occupancy(a, vec, &per_sm) != cudaSuccess) return HPTT_ERR_CUDA;
-  if (launch_single(a, vec, 0, s) != cudaSuccess) return HPTT_ERR_CUDA;
+  int per_sm = 0, sms = 0;
+  if (occupancy(a, vec, &per_sm) != cudaSuccess ||
+      cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess)
+    return HPTT_ERR_CUDA;
+  // the persistent TMA tile's grid: the resident CTAs (other kernels run one
+  // CTA per tile)
+  if (launch_single(a, vec, per_sm * sms, s) != cudaSuccess) return HPTT_ERR_CUDA;
   return HPTT_OK;
 }
 

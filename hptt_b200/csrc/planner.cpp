@@ -729,7 +729,82 @@ int choose_vtile(const HpttProblem &p, const TileParams &tp, int update, HpttTil
   return t->num_tiles ? ST_OK : ST_TOO_LARGE;
 }
 
+// TMA tile (KIND_TTILE, ttile.cuh): tkx x tky boxes of 128 / sizeof(E)
+// elements on each side, one grid level per tile position.
+int choose_ttile(const HpttProblem &p, const TileParams &tp, int update, HpttTile *t) {
+  if (!ttile_possible(p)) return ST_TOO_LARGE;
+  const int sz = elem_bytes(p.dtype);
+  const int box = 128 / sz;
+  const int kx = tp.tt_kx, ky = tp.tt_ky;
+  if (kx < 1 || ky < 1 || kx * ky > 8 || tp.tt < 1 || tp.tt > 4) return ST_TOO_LARGE;
+  std::memset(t, 0, sizeof(*t));
+  t->kind = KIND_TTILE;
+  t->nt = 64 * kx * ky;
+  if (tp.tt >= 2) {
+    if (kx * ky > 4) return ST_TOO_LARGE;  // the persistent build's thread limit
+    t->nt += 32;                           // the producer warp
+  }
+  t->W = 1;
+  t->xc = t->yc = t->wc = -1;
+  const int p0 = p.perm[0];
+  t->nx = t->ny = 1;
+  t->xd[0] = 0;
+  t->yd[0] = p0;
+  t->TX = kx * box;
+  t->TY = ky * box;
+  t->xt[0] = t->TX;
+  t->yt[0] = t->TY;
+  t->tkx = kx;
+  t->tky = ky;
+  t->ts = tp.tt >= 2 ? tp.tt : 0;
+  int64_t tile_ext[HPTT_MAX_RANK];
+  for (int d = 0; d < p.rank; ++d) tile_ext[d] = 1;
+  tile_ext[0] = t->TX;
+  tile_ext[p0] = t->TY;
+  finish_grid(p, t, tile_ext, {0, p0}, tp.grid_order);
+  // one CTA per tile: A's and B's boxes, the mbarrier (16 bytes at the
+  // base) and the slack that aligns the boxes to the 128-byte swizzle's
+  // 1024-byte pattern; persistent CTAs: ts stages of A's boxes (and B's when
+  // B is read), three output buffers of boxes, a 256-byte header (mbarriers
+  // and tile origins) and the same slack
+  const int kb = kx * ky * box * 128;
+  t->smem_bytes = t->ts ? t->ts * kb * (update ? 2 : 1) + 3 * kb + 1024 + 256
+                        : 2 * kb + 1024 + 16;
+  if (t->smem_bytes > 227 * 1024) return ST_TOO_LARGE;  // sm_100a's per-CTA limit
+  t->tab2_off = 16;
+  t->thr_off = 16;
+  t->table_bytes = 16;
+  return t->num_tiles ? ST_OK : ST_TOO_LARGE;
+}
+
 }  // namespace
+
+bool ttile_possible(const HpttProblem &p) {
+  const int sz = elem_bytes(p.dtype);
+  if ((sz != 4 && sz != 8) || p.rank < 2 || p.rank > 5 || p.perm[0] == 0) return false;
+  for (int d = 0; d < p.rank; ++d) {
+    if (p.n[d] < 1 || p.n[d] > 0xffffffffLL) return false;
+    if (d > 0 && ((p.sA[d] * sz) % 16 != 0 || p.sA[d] * sz >= (int64_t(1) << 40))) return false;
+    if (d != p.perm[0] && ((p.sB[d] * sz) % 16 != 0 || p.sB[d] * sz >= (int64_t(1) << 40)))
+      return false;
+  }
+  return p.sA[0] == 1 && p.sB[p.perm[0]] == 1;
+}
+
+int ttile_map_params(const HpttProblem &p, const HpttTile &t, int side, TtileMapParams *out) {
+  if (t.kind != KIND_TTILE || !ttile_possible(p)) return ST_TOO_LARGE;
+  const int sz = elem_bytes(p.dtype);
+  const uint32_t box = 128 / sz;
+  out->rank = p.rank;
+  out->elem_bytes = sz;
+  for (int k = 0; k < p.rank; ++k) {
+    const int d = side == 0 ? k : p.perm[k];  // input dim of this map dim
+    out->dims[k] = static_cast<uint64_t>(p.n[d]);
+    out->stride_bytes[k] = static_cast<uint64_t>(side == 0 ? p.sA[d] : p.sB[d]) * sz;
+    out->box[k] = d == 0 ? box : (d == p.perm[0] ? box : 1u);
+  }
+  return ST_OK;
+}
 
 bool vtile_possible(const HpttProblem &p) {
   const int sz = elem_bytes(p.dtype);
@@ -756,6 +831,7 @@ int choose_tile(const HpttProblem &p, const TileParams &tp, int update, HpttTile
   if (r == 1 || (common && p.n[0] * sz >= tp.rows_min_bytes))
     return choose_rows(p, tp, t);
   if (common && p.n[0] > tp.nt / 2) return choose_rows(p, tp, t);
+  if (tp.tt && ttile_possible(p) && choose_ttile(p, tp, update, t) == ST_OK) return ST_OK;
   if (tp.vt && vtile_possible(p) && choose_vtile(p, tp, update, t) == ST_OK) return ST_OK;
 
   std::memset(t, 0, sizeof(*t));
@@ -1049,9 +1125,14 @@ std::string describe(const HpttProblem &p, const HpttTile &t) {
   os << "\nkernel: "
      << (t.kind == KIND_TILE    ? "tile (shared-memory transpose)"
          : t.kind == KIND_VTILE ? "vector tile (16-byte windows, shared-memory transpose)"
+         : t.kind == KIND_TTILE ? "TMA tile (tensor-map box loads and stores, shared-memory transpose)"
                                 : "rows (shared stride-1)")
      << ", " << t.nt << " threads/CTA";
   if (t.kind == KIND_ROWS) os << ", vector " << t.vec;
+  if (t.kind == KIND_TTILE) {
+    os << ", boxes " << t.tkx << " x " << t.tky;
+    if (t.ts) os << ", persistent, " << t.ts << " stages";
+  }
   if (t.kind == KIND_VTILE)
     os << ", slots " << (8 << t.vlx) << " x " << (8 << t.vly) << ", J " << t.J1 << "/" << t.J2
        << ", " << t.vj << " vectors/thread" << (t.vpre ? ", B read first" : "");

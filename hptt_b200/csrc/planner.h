@@ -65,7 +65,29 @@ struct TileParams {
                            // phase: 8 (64 registers) or 4 (32 registers)
   int vt_pre = 0;          // 1: update tiles with vt_j == 4 read B before A
                            // (64 registers)
+  int tt = 0;              // a TMA tile (KIND_TTILE) where the shape allows
+                           // one (takes precedence over vt): 1 = one CTA per
+                           // tile, 2-4 = persistent CTAs with tt stages
+  int tt_kx = 2;           // boxes per TMA tile along input dim 0 and along
+  int tt_ky = 2;           // the output's leading dim (64 threads per box)
 };
+
+// Whether a TMA tile (KIND_TTILE) can serve this problem: fused rank 2-5,
+// 4- or 8-byte elements, no shared stride-1 dim, every stride other than the
+// unit one a multiple of 16 bytes and below 2^40 bytes, extents below 2^32.
+bool ttile_possible(const HpttProblem &p);
+
+// The tensor map of one side of a KIND_TTILE tile: side 0 is A with its dims
+// in input order, side 1 is B with its dims in output order.  stride_bytes[0]
+// is the element size; box = the tile's box extents (1 outside the box).
+struct TtileMapParams {
+  int rank = 0;
+  int elem_bytes = 0;
+  uint64_t dims[5] = {0};
+  uint64_t stride_bytes[5] = {0};
+  uint32_t box[5] = {0};
+};
+int ttile_map_params(const HpttProblem &p, const HpttTile &t, int side, TtileMapParams *out);
 
 // Whether a vector tile (KIND_VTILE) can serve this problem: elements of at
 // most 8 bytes and no shared stride-1 dim.

@@ -28,6 +28,8 @@ void build_typed(const HpttProblem &P, const HpttTile &T, unsigned char *base) {
     }
     HpttThr *thr = reinterpret_cast<HpttThr *>(base + T.thr_off);
     for (int t = 0; t < T.nt; ++t) thr[t] = tile_thread_consts(P, T, m, t);
+  } else if (T.kind == KIND_TTILE) {
+    // no tables: TMA addresses both tensors from the tile coordinates
   } else if (T.kind == KIND_VTILE) {
     std::vector<int64_t> rowA, colB;
     vtile_maps(P, T, &rowA, &colB);

@@ -17,6 +17,7 @@
 #include "kernels.cuh"
 #include "planner.h"
 #include "tables.h"
+#include "ttile.cuh"
 #include "vtile.cuh"
 
 namespace hptt_b200 {
@@ -439,6 +440,86 @@ int replay_vtile(const HpttProblem &P, const HpttTile &T, int update, const Layo
   return 0;
 }
 
+// TMA tile (ttile.cuh): both tensor maps as the launcher encodes them
+// (ttile_map_params), checked against the rules TMA imposes -- unit element
+// stride innermost, other strides multiples of 16 bytes, 128-byte inner box
+// rows, innermost coordinates of every load and store multiples of 16
+// bytes, no negative coordinate -- then every box of every tile, clipped at
+// the tensor's edges as TMA clips it, with A and B addresses computed from
+// the maps: every inner element of B written exactly once, with the element
+// of A the permutation maps to it.  (The persistent form walks tiles
+// blockIdx.x + i * gridDim.x, each tile once for any grid, so the same
+// per-tile check covers it.)
+int replay_ttile(const HpttProblem &P, const HpttTile &T, const Layout &L, int update,
+                 std::vector<uint8_t> &writes, uint64_t *checked) {
+  const int esz = elem_bytes(P.dtype);
+  const int BOX = 128 / esz;
+  TtileMapParams ma, mb;
+  if (ttile_map_params(P, T, 0, &ma) != ST_OK || ttile_map_params(P, T, 1, &mb) != ST_OK)
+    return 401;
+  if (ma.rank != P.rank || mb.rank != P.rank || ma.rank > 5) return 402;
+  if (ma.stride_bytes[0] != static_cast<uint64_t>(esz) ||
+      mb.stride_bytes[0] != static_cast<uint64_t>(esz))
+    return 403;
+  uint64_t boxa = 1, boxb = 1;
+  for (int k = 0; k < P.rank; ++k) {
+    if (k > 0 && (ma.stride_bytes[k] % 16 || mb.stride_bytes[k] % 16)) return 404;
+    boxa *= ma.box[k];
+    boxb *= mb.box[k];
+  }
+  if (ma.box[0] * esz != 128 || mb.box[0] * esz != 128) return 405;
+  if (boxa != static_cast<uint64_t>(BOX) * BOX || boxb != boxa) return 406;
+  const int K = T.tkx * T.tky;
+  if (K < 1 || K > 8 || (!T.ts && T.nt != 64 * K)) return 407;
+  // shared memory: one CTA per tile, two boxes per box of the tile; the
+  // persistent form, ts stages (A's boxes, and B's when B is read) and three
+  // output buffers; both with the header and alignment slack
+  const int kb = K * BOX * 128;
+  const int64_t need = T.ts ? int64_t(T.ts) * kb * (update ? 2 : 1) + 3 * kb + 1024 + 256
+                            : 2 * kb + 1024 + 16;
+  if (T.ts < 0 || T.ts == 1 || T.ts > 4 || T.smem_bytes < need) return 408;
+  if (T.ts && (K > 4 || T.nt != 64 * K + 32)) return 415;
+  const int p0 = P.perm[0];
+  for (uint32_t tile = 0; tile < T.num_tiles; ++tile) {
+    int32_t org[5];
+    ttile_coords(T, tile, org);
+    for (int g = 0; g < K; ++g) {
+      int32_t ca[5], cb[5];
+      for (int d = 0; d < 5; ++d) ca[d] = org[d];
+      ca[0] += (g % T.tkx) * BOX;
+      ca[p0] += (g / T.tkx) * BOX;
+      if (!(ca[0] < P.n[0] && ca[p0] < P.n[p0])) continue;  // the kernel skips it
+      for (int k = 0; k < P.rank; ++k) cb[k] = ca[P.perm[k]];
+      for (int k = 0; k < P.rank; ++k)
+        if (ca[k] < 0 || cb[k] < 0) return 409;
+      if ((static_cast<int64_t>(ca[0]) * esz) % 16 || (static_cast<int64_t>(cb[0]) * esz) % 16)
+        return 410;
+      for (int y = 0; y < BOX; ++y) {
+        for (int x = 0; x < BOX; ++x) {
+          int64_t c[5];
+          for (int d = 0; d < P.rank; ++d) c[d] = ca[d];
+          c[0] += x;
+          c[p0] += y;
+          if (c[0] >= P.n[0] || c[p0] >= P.n[p0]) continue;  // clipped by TMA
+          uint64_t oa = 0, ob = 0;
+          for (int k = 0; k < P.rank; ++k) {
+            oa += static_cast<uint64_t>(c[k]) * ma.stride_bytes[k];
+            ob += static_cast<uint64_t>(c[P.perm[k]]) * mb.stride_bytes[k];
+          }
+          const int64_t ia = static_cast<int64_t>(oa / esz), ib = static_cast<int64_t>(ob / esz);
+          if (ia < 0 || ia >= L.nA) return 411;
+          if (ib < 0 || ib >= L.nB) return 412;
+          if (map_a_to_b(L, ia) != ib) return 413;
+          if (writes[ib] != 0) return 414;
+          writes[ib] = 1;
+          ++*checked;
+        }
+      }
+    }
+  }
+  return 0;
+}
+
 template <typename OffT>
 int replay_rows(const HpttProblem &P, const HpttTile &T, const Layout &L,
                 const std::vector<unsigned char> &tab, std::vector<uint8_t> &writes,
@@ -629,6 +710,31 @@ extern "C" int hptt_cuda_debug_check_indexing(int dtype, uint32_t rank, const ui
           if (checked && *checked != n) return 2301;
         }
       }
+    }
+  }
+  // TMA tiles: boxes per tile and both grid orders
+  if (ttile_possible(P)) {
+    // (boxes along input dim 0, along the output's leading dim, grid order,
+    // stages, B read)
+    const int forms[][5] = {{1, 1, 0, 1, 0}, {2, 2, 1, 1, 1}, {4, 2, 0, 1, 0}, {1, 4, 1, 2, 1},
+                            {2, 1, 0, 4, 0}, {1, 1, 0, 3, 1}, {2, 2, 1, 2, 0}};
+    for (const auto &f : forms) {
+      TileParams tp2;
+      tp2.tt = f[3];
+      tp2.tt_kx = f[0];
+      tp2.tt_ky = f[1];
+      tp2.grid_order = f[2];
+      HpttTile T;
+      st = choose_tile(P, tp2, f[4], &T);
+      if (st != ST_OK) return st;
+      if (T.kind != KIND_TTILE) return 2400;
+      std::vector<uint8_t> writes(static_cast<size_t>(L.nB), 0);
+      uint64_t n = 0;
+      const int rc = replay_ttile(P, T, L, f[4], writes, &n);
+      if (rc != 0) return 2000 + rc;
+      for (int64_t ib = 0; ib < L.nB; ++ib)
+        if (writes[ib] != inner[ib]) return 2401;
+      if (checked && *checked != n) return 2402;
     }
   }
   return 0;

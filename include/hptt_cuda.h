@@ -177,6 +177,12 @@ int hptt_cuda_debug_check_vtile(int dtype, uint32_t rank, const uint32_t *in_siz
                                 int vj, int grid_order, int update, int mis_a, int mis_b,
                                 uint64_t *checked);
 
+/* CTAs of TMA-tile launches (KIND_TTILE) whose bounded wait for their box
+ * loads ran out since the library was loaded on the current device; such a
+ * CTA stores nothing.  0 in every correct run.  Extension, for tests; no
+ * reference counterpart. */
+int hptt_cuda_debug_tma_timeouts(uint32_t *count);
+
 /* Size of the fixed device array hptt_cuda_transpose_noalloc keeps its
  * offset tables in (one array per GPU, held until the process exits). */
 #define HPTT_NOALLOC_TABLE_BYTES 65536

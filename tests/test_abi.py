@@ -141,10 +141,10 @@ def test_tune_cache_round_trip(tmp_path):
     out = tmp_path / "out.cache"
     h.tune_cache_save(str(out))
     lines = sorted(out.read_text().splitlines())
-    assert lines == ["NVIDIA B200 0 2 1,0 27 0|256 16384 32768 512 0 0 0 1 1 256 0 0 16 16 8 0",
-                     "NVIDIA B200 0 3 2,1,0 27 1|256 16384 32768 512 0 0 0 1 1 256 0 1 32 8 4 0",
-                     "NVIDIA B200 0 4 2,3,0,1 27 1|256 16384 32768 512 0 0 1 0 1 256 0 0 16 16 8 0",
-                     "NVIDIA B200 1 3 2,0,1 28 1|128 8192 32768 512 1 4 0 1 1 256 0 0 16 16 8 0"]
+    assert lines == ["NVIDIA B200 0 2 1,0 27 0|256 16384 32768 512 0 0 0 1 1 256 0 0 16 16 8 0 0 2 2",
+                     "NVIDIA B200 0 3 2,1,0 27 1|256 16384 32768 512 0 0 0 1 1 256 0 1 32 8 4 0 0 2 2",
+                     "NVIDIA B200 0 4 2,3,0,1 27 1|256 16384 32768 512 0 0 1 0 1 256 0 0 16 16 8 0 0 2 2",
+                     "NVIDIA B200 1 3 2,0,1 28 1|128 8192 32768 512 1 4 0 1 1 256 0 0 16 16 8 0 0 2 2"]
     h.tune_cache_clear()
     assert h.tune_cache_size() == 0
     with pytest.raises(h.HpttError):

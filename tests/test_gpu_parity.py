@@ -280,11 +280,12 @@ def test_tile_forms_match(tmp_path, name, size, perm, al, be):
         (line,) = path.read_text().splitlines()
         key, fields = line.split("|")
         f = fields.split()
-        assert len(f) == 16
+        assert len(f) == 19
         for walk, exact, nt, order in ((0, 0, 256, 0), (0, 1, 256, 0), (1, 0, 256, 0),
                                        (1, 1, 256, 1), (1, 1, 512, 0), (0, 0, 512, 1)):
             f[7], f[8], f[9], f[10] = str(walk), str(exact), str(nt), str(order)
             f[11] = "0"  # the shared-memory tile forms, not the vector tile
+            f[16] = "0"  # nor the TMA tile
             path.write_text(key + "|" + " ".join(f) + "\n")
             h.tune_cache_clear()
             h.tune_cache_load(str(path))

@@ -174,3 +174,38 @@ def test_replay_vtile_every_tuner_form(dt, size, perm):
                         assert n in (0, np.prod(size))
                         used += n > 0
     assert used > 0, "no vector tile planned"
+
+
+# Shapes a TMA tile can serve (every stride other than the unit one a
+# multiple of 16 bytes, fused rank <= 5), with extents that are not
+# multiples of the 128-byte boxes: the debug replay adds the TMA-tile forms
+# for these, with both tensor maps checked against TMA's rules.
+TTILE_SHAPES = [
+    ("f32", [64, 48, 20], [2, 1, 0]),
+    ("f32", [100, 36, 60], [1, 0, 2]),
+    ("f64", [30, 18, 8], [2, 0, 1]),
+    ("c64", [16, 5, 6, 10], [3, 1, 0, 2]),
+    ("f32", [4, 8, 3, 5, 12], [4, 2, 0, 1, 3]),
+    ("f32", [256, 256, 16], [2, 1, 0]),
+    ("f32", [1000, 332], [1, 0]),
+    ("f64", [258, 130], [1, 0]),
+    ("f32", [8, 3, 4, 5, 4], [4, 2, 0, 3, 1]),  # fused rank 5
+]
+
+
+@pytest.mark.parametrize("dt,size,perm", TTILE_SHAPES)
+def test_replay_ttile_shapes(dt, size, perm):
+    assert "TMA" not in h.inspect_plan(dt, size, perm)  # not the default plan
+    rc, n = check(dt, size, perm)
+    assert rc == 0, (dt, size, perm, rc)
+    assert n == np.prod(size)
+
+
+def test_replay_ttile_outer_sizes():
+    """Sub-tensors: outer extents keep the strides 16-byte multiples (and
+    pass the reference's guard, which also wants out_outer[perm[i]] >=
+    in_size[i])."""
+    rc, n = check("f32", [40, 20, 12], [2, 0, 1], [44, 24, 12], [20, 40, 40])
+    assert rc == 0 and n == 40 * 20 * 12
+    rc, n = check("c64", [6, 10, 7], [1, 2, 0], [8, 10, 9], [12, 7, 10])
+    assert rc == 0 and n == 6 * 10 * 7

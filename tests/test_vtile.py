@@ -67,13 +67,13 @@ def _cache_line(tmp_path, name, size, perm, al, be, cs):
     (line,) = path.read_text().splitlines()
     key, fields = line.split("|")
     f = fields.split()
-    assert len(f) == 16
+    assert len(f) == 19
     return path, key, f
 
 
 def _force(path, key, f, nt, nvx, nvy, order, vj=8, pre=0):
     g = list(f)
-    g[9:16] = [str(nt), str(order), "1", str(nvx), str(nvy), str(vj), str(pre)]
+    g[9:17] = [str(nt), str(order), "1", str(nvx), str(nvy), str(vj), str(pre), "0"]
     path.write_text(key + "|" + " ".join(g) + "\n")
     h.tune_cache_clear()
     h.tune_cache_load(str(path))
