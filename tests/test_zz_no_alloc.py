@@ -107,3 +107,53 @@ def test_noalloc_rejects_bad_arguments():
     size_fn = h.load_library().hptt_cuda_noalloc_table_bytes
     size_fn.restype = ctypes.c_size_t
     assert size_fn() == 65536
+
+
+def test_noalloc_tma_tile_from_cache(tmp_path):
+    """A tune-cache entry that names the TMA tile: the allocation-free call
+    runs it (persistent and one-CTA-per-tile forms) on 16-byte aligned bases
+    and plans the element tile on bases one element off, equal to the oracle
+    either way."""
+    name, size, perm, al, be = "f32", [100, 36, 60], [1, 0, 2], 2.3, 4.2
+    esz = 4
+    rng = np.random.default_rng(29)
+    n_in, n_out = footprint(size, perm)
+    a = seeded(rng, n_in, name)
+    b0 = seeded(rng, n_out, name)
+    want = oracle_run(name, size, perm, al, be, a, b0)
+    h.tune_cache_clear()
+    try:
+        x = torch.zeros(n_in, dtype=torch.float32, device="cuda")
+        y = torch.zeros(n_out, dtype=torch.float32, device="cuda")
+        p = h.create_plan(x, y, size, perm, al, be, 1, 2e-3, dtype=name)
+        assert p is not None
+        p.destroy()
+        path = tmp_path / "noalloc_tt.cache"
+        h.tune_cache_save(str(path))
+        (line,) = path.read_text().splitlines()
+        key, fields = line.split("|")
+        f = fields.split()
+        assert len(f) == 19
+        for stages, kx, ky in ((1, 2, 1), (3, 1, 1)):
+            f[10], f[11] = "0", "0"
+            f[16:19] = [str(stages), str(kx), str(ky)]
+            path.write_text(key + "|" + " ".join(f) + "\n")
+            h.tune_cache_clear()
+            h.tune_cache_load(str(path))
+            for offset in (0, 1):
+                da = torch.empty(n_in + offset, dtype=torch.float32, device="cuda")
+                db = torch.empty(n_out + offset, dtype=torch.float32, device="cuda")
+                da[offset:].copy_(torch.from_numpy(a))
+                db[offset:].copy_(torch.from_numpy(b0))
+                alpha = (ctypes.c_double * 2)(al, 0.0)
+                beta = (ctypes.c_double * 2)(be, 0.0)
+                stream = torch.cuda.current_stream()
+                rc = _noalloc_fn()(h.dtype_code(name), len(size), _u32(size), _u32(perm), None,
+                                   None, alpha, beta, 0, da[offset:].data_ptr(),
+                                   db[offset:].data_ptr(), stream.cuda_stream)
+                assert rc == 0
+                stream.synchronize()
+                assert_same(db[offset:].cpu().numpy(), want, name,
+                            f"stages={stages} boxes={kx}x{ky} offset={offset * esz} B")
+    finally:
+        h.tune_cache_clear()
