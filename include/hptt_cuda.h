@@ -156,8 +156,12 @@ int hptt_cuda_plan_inspect(int dtype, uint32_t rank, const uint32_t *in_size,
  * every access stays inside the buffers and shared memory, and that every
  * inner element of B is written exactly once with the element of A the
  * permutation maps to it.  max_vec_bytes limits vector accesses (0 = widest).
- * Returns 0 when all checks hold, else a diagnostic code >= 1000.  Extension,
- * for tests; no reference counterpart. */
+ * Where the problem allows them, it then replays vector-tile forms the tuner
+ * tries (bases on and off a 16-byte boundary) and TMA-tile forms (both
+ * tensor maps checked against TMA's stride, box and coordinate rules, every
+ * box clipped at the tensor's edges).  Returns 0 when all checks hold, else
+ * a diagnostic code >= 1000.  Extension, for tests; no reference
+ * counterpart. */
 int hptt_cuda_debug_check_indexing(int dtype, uint32_t rank, const uint32_t *in_size,
                                    const uint32_t *perm, const uint32_t *in_outer,
                                    const uint32_t *out_outer, int max_vec_bytes,
