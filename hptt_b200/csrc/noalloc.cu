@@ -12,15 +12,12 @@
 //
 // The array is a file-scope __device__ variable of HPTT_NOALLOC_TABLE_BYTES
 // bytes; every GPU that loads the library holds it until the process exits.
-// In host code its name only stands in for it, so its device address is
-// looked up once per device, with that device current, by
-// cudaGetSymbolAddress, and that address is what the kernel receives.  The
-// address is kept for the life of the process: after cudaDeviceReset (which
-// destroys the context that holds the array) this entry point must not be
-// called again in that process.
+// In host code its name only stands in for it, so every call looks its
+// device address up in the current context with cudaGetSymbolAddress, and
+// that address is what the kernel receives (so the call keeps working after
+// cudaDeviceReset re-creates the context).
 #include <cuda_runtime.h>
 
-#include <mutex>
 #include <vector>
 
 #include "../../include/hptt_cuda.h"
@@ -35,25 +32,18 @@ namespace {
 
 static __device__ __align__(256) unsigned char g_noalloc_tables[HPTT_NOALLOC_TABLE_BYTES];
 
-constexpr int kMaxDevices = 64;
-std::mutex g_mu;
-void *g_table_ptr[kMaxDevices] = {nullptr};
-
-// Device address of g_noalloc_tables on `device` (the current device),
-// looked up on the first call for that device.
+// Device address of g_noalloc_tables in the current context, looked up on
+// every call (a host-side query; a cached address would outlive a context
+// torn down by cudaDeviceReset).
 int table_address(int device, void **out) {
-  if (device < 0 || device >= kMaxDevices) return ST_NO_DEVICE;
-  std::lock_guard<std::mutex> lk(g_mu);
-  if (!g_table_ptr[device]) {
-    void *ptr = nullptr;
-    const cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_tables);
-    if (e != cudaSuccess || !ptr) {
-      cudaGetLastError();
-      return ST_CUDA;
-    }
-    g_table_ptr[device] = ptr;
+  if (device < 0) return ST_NO_DEVICE;
+  void *ptr = nullptr;
+  const cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_tables);
+  if (e != cudaSuccess || !ptr) {
+    cudaGetLastError();
+    return ST_CUDA;
   }
-  *out = g_table_ptr[device];
+  *out = ptr;
   return ST_OK;
 }
 

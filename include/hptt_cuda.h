@@ -215,10 +215,8 @@ int hptt_cuda_debug_tma_timeouts(uint32_t *count);
  * The array is shared by every call in the process on that GPU and keeps
  * the last call's tables: calls that can run at the same time on the GPU
  * (different streams, several host threads) race on it and must be
- * serialised by the caller; calls on one stream are ordered.  The first call
- * on each device looks the array's address up (a one-time set-up, kept for
- * the life of the process; after cudaDeviceReset the call must not be used
- * again in that process).
+ * serialised by the caller; calls on one stream are ordered.  Each call
+ * looks the array's address up in the current context.
  */
 int hptt_cuda_transpose_noalloc(int dtype, uint32_t rank, const uint32_t *in_size,
                                 const uint32_t *perm, const uint32_t *in_outer,
