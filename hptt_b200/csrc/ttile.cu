@@ -16,8 +16,9 @@ using namespace dev;
 
 namespace {
 
-// Waits that ran out (ttile_wait): counted per launch site, read by
-// hptt_cuda_debug_tma_timeouts.  A timed-out CTA stores nothing.
+// CTAs whose bounded wait (ttile_wait) ran out, counted on each device since
+// the library was loaded, read by hptt_cuda_debug_tma_timeouts.  A timed-out
+// CTA stores nothing.
 __device__ unsigned int g_ttile_timeouts = 0;
 
 // try_wait polls before a CTA gives up on its loads.
@@ -108,10 +109,14 @@ __global__ void __launch_bounds__(512)
       if (UPD) ttile_load(&mapB, smem_addr(bufB + g * BOXB), sbar, rank, cb);
     }
   }
-  // every thread waits; if any gave up, the whole CTA stores nothing
+  // every thread waits; if any gave up, the whole CTA stores nothing, and
+  // thread 0 waits once more (bounded) for the loads still in flight
   const bool timed_out = !ttile_wait(sbar, 0, kWaitPolls);
   if (__syncthreads_or(timed_out)) {
-    if (tid == 0) atomicAdd(&g_ttile_timeouts, 1u);
+    if (tid == 0) {
+      atomicAdd(&g_ttile_timeouts, 1u);
+      ttile_wait(sbar, 0, kWaitPolls);
+    }
     return;
   }
   const Scal sc{args.alpha[0], args.alpha[1], args.beta[0], args.beta[1]};

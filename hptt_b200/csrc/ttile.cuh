@@ -24,14 +24,16 @@
 //   3. after a proxy fence and a barrier, one thread issues one TMA store per
 //      box and waits until the stores have read shared memory.
 // Persistent form (HpttTile::ts = S stages): a grid of resident CTAs walks
-// the tiles (tile blockIdx.x + i gridDim.x), and a CTA keeps its next S
-// tiles' loads in flight in a ring of S stages, one mbarrier each (phase
-// parity (i / S) & 1 for its i-th tile).  The transposed boxes go to one of
-// two output buffers, which the TMA stores read while the CTA works on the
-// next tile; before a buffer is written again, the stores issued from it two
-// tiles earlier have read it (cp.async.bulk.wait_group.read 1).  A stage is
-// reloaded (tile i + S) once every thread has passed the barrier after
-// reading it.
+// the tiles (tile blockIdx.x + i gridDim.x), warp-specialised.  A producer
+// lane keeps the CTA's next S tiles' loads in flight in a ring of S stages,
+// each with a "full" mbarrier (armed with the tile's bytes; phase parity
+// (i / S) & 1 for the CTA's i-th tile) and an "empty" one the consumers
+// arrive on once they have read the stage.  The consumer threads (64 per
+// box) transpose into one of three output buffers, which the TMA stores read
+// while the next tiles are transposed: before the consumers' barrier of
+// tile i, their thread 0 waits until at most one store group is still
+// reading shared memory (cp.async.bulk.wait_group.read 1), so the buffer of
+// tile i - 2 is free for tile i + 1.
 //
 // TMA clips at the tensor's edges (loads fill zeros outside, stores skip
 // them), so edge tiles need no code of their own.  The innermost coordinate
