@@ -651,7 +651,7 @@ def run_served(args, plans):
     rates = [float(r) for r in args.serve_rates.split(",")]
     keys = ("submitted", "completed", "launches", "mean_batch", "throughput_rps", "gbs",
             "lat_p50_us", "lat_p99_us", "lat_p999_us", "lat_max_us", "peak_inflight_bytes",
-            "peak_pending")
+            "peak_pending", "sched_pass_max_us")
     out = {"budget_bytes": budget, "seconds_per_rate": args.serve_seconds,
            "pool": len(plans), "rates": []}
     for mode in ("batched", "per_call"):

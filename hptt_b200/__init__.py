@@ -78,7 +78,8 @@ class ServeStats(ctypes.Structure):
                     "peak_inflight_bytes", "peak_pending")] + \
                [(n, ctypes.c_double) for n in (
                     "elapsed_s", "throughput_rps", "gbs", "mean_batch", "lat_mean_us",
-                    "lat_p50_us", "lat_p99_us", "lat_p999_us", "lat_max_us")]
+                    "lat_p50_us", "lat_p99_us", "lat_p999_us", "lat_max_us",
+                    "sched_pass_max_us")]
 
     def as_dict(self):
         return {name: getattr(self, name) for name, _ in self._fields_}

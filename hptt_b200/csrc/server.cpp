@@ -128,6 +128,7 @@ struct Server {
   uint64_t submitted = 0, completed = 0, failed = 0, launches = 0, bytes_done = 0;
   uint64_t batched_requests = 0;
   uint64_t peak_inflight_bytes = 0, peak_pending = 0;
+  double loop_max_us = 0;              // longest scheduler pass (no idle wait)
   Clock::time_point t_first_submit, t_last_done;
   bool have_first = false;
 
@@ -340,9 +341,17 @@ void fail_queued(Server *s) {
 void worker_main(Server *s) {
   cudaSetDevice(s->device);
   const size_t max_batch = s->cfg.per_call ? 1 : std::max<uint32_t>(1, s->cfg.max_batch);
+  // start of the current pass of the loop (reset after an idle wait), for
+  // the longest-pass statistic: a pass that takes long means this thread was
+  // held up, in a CUDA call or off the CPU
+  Clock::time_point t_pass = Clock::now();
   for (;;) {
     {
+      const Clock::time_point now = Clock::now();
       std::lock_guard<std::mutex> lk(s->mu);
+      s->loop_max_us = std::max(s->loop_max_us,
+                                std::chrono::duration<double, std::micro>(now - t_pass).count());
+      t_pass = now;
       while (!s->incoming.empty()) {
         enqueue_request(s, s->incoming.front());
         s->incoming.pop_front();
@@ -447,6 +456,7 @@ void worker_main(Server *s) {
     if (!busy && s->incoming.empty()) {
       // idle: sleep until a submission (or stop)
       s->cv_submit.wait_for(lk, std::chrono::milliseconds(5));
+      t_pass = Clock::now();
     } else {
       lk.unlock();
       std::this_thread::yield();
@@ -644,6 +654,7 @@ int hptt_cuda_server_stats(hptt_cuda_server_t server, hptt_cuda_serve_stats *out
     out->bytes = s->bytes_done;
     out->peak_inflight_bytes = s->peak_inflight_bytes;
     out->peak_pending = s->peak_pending;
+    out->sched_pass_max_us = s->loop_max_us;
     out->mean_batch = s->launches ? static_cast<double>(s->batched_requests) / s->launches : 0;
     if (s->have_first && s->completed)
       out->elapsed_s = std::chrono::duration<double>(s->t_last_done - s->t_first_submit).count();
@@ -676,6 +687,7 @@ int hptt_cuda_server_reset_stats(hptt_cuda_server_t server) {
   s->submitted = s->completed = s->failed = s->launches = s->bytes_done = 0;
   s->batched_requests = 0;
   s->peak_inflight_bytes = s->peak_pending = 0;
+  s->loop_max_us = 0;
   s->have_first = false;
   return HPTT_OK;
 }

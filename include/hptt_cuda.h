@@ -311,6 +311,9 @@ typedef struct {
   uint64_t peak_inflight_bytes, peak_pending;
   double elapsed_s, throughput_rps, gbs, mean_batch;
   double lat_mean_us, lat_p50_us, lat_p99_us, lat_p999_us, lat_max_us;
+  double sched_pass_max_us;  /* longest pass of the scheduler thread's loop
+                                (idle waits excluded): a long one means the
+                                thread was held up */
 } hptt_cuda_serve_stats;
 int hptt_cuda_server_create(const hptt_cuda_serve_config *cfg, hptt_cuda_server_t *server);
 int hptt_cuda_server_submit(hptt_cuda_server_t server, hptt_cuda_plan_t plan, const void *in,
