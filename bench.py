@@ -198,7 +198,8 @@ def _make_plans(cases, rank):
         d = p.describe()
         kind = ("rows" if "kernel: rows" in d else
                 "vtile" if "kernel: vector tile" in d else
-                "ttile" if "kernel: TMA tile" in d else "tile")
+                ("ttile_pipe" if "persistent" in d else "ttile") if "kernel: TMA tile" in d else
+                "tile")
         plans.append((p, algorithmic_bytes(c), kind, c))
     torch.cuda.synchronize()
     return plans, bufs
@@ -275,7 +276,8 @@ def _timed_steps(plans, steps, warmup, stream, dist, world, flush=None):
     return elapsed_ms, kind_ms, clocks
 
 
-KERNEL_OF_KIND = {"tile": "k_tile", "vtile": "k_vtile", "ttile": "k_ttile", "rows": "k_rows"}
+KERNEL_OF_KIND = {"tile": "k_tile", "vtile": "k_vtile", "ttile": "k_ttile",
+                  "ttile_pipe": "k_ttile_pipe", "rows": "k_rows"}
 
 
 def _roofline(plans, kind_ms, steps, traffic=None):
