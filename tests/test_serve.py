@@ -121,4 +121,6 @@ def test_budget_rejects_oversize_and_poisson_smoke():
     assert st["submitted"] > 1000 and st["completed"] == st["submitted"]
     assert st["failed"] == 0
     assert 0 < st["lat_p50_us"] <= st["lat_p99_us"] <= st["lat_p999_us"] <= st["lat_max_us"]
+    # the scheduler thread's longest pass: some time, and no longer than the run
+    assert 0 < st["sched_pass_max_us"] <= st["elapsed_s"] * 1e6 + 1e6
     srv.destroy()
