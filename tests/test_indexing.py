@@ -209,3 +209,44 @@ def test_replay_ttile_outer_sizes():
     assert rc == 0 and n == 40 * 20 * 12
     rc, n = check("c64", [6, 10, 7], [1, 2, 0], [8, 10, 9], [12, 7, 10])
     assert rc == 0 and n == 6 * 10 * 7
+
+
+def _random_ttile_case(seed):
+    """A seeded problem a TMA tile can serve: no extent-1 dims, input dim 0
+    and the output's leading dim in multiples of 16 bytes, so every stride
+    other than the unit one is a 16-byte multiple (fusion can only merge such
+    dims into longer ones)."""
+    rng = np.random.default_rng(seed)
+    dt = ["f32", "f64", "c64"][seed % 3]
+    q = 4 if dt == "f32" else 2  # elements per 16 bytes
+    rank = int(rng.integers(2, 6))
+    while True:
+        perm = [int(x) for x in rng.permutation(rank)]
+        if perm[0] != 0:
+            break
+    size = [int(rng.integers(2, 9)) for _ in range(rank)]
+    size[0] = q * int(rng.integers(1, 12))
+    size[perm[0]] = q * int(rng.integers(1, 12))
+    return dt, size, perm
+
+
+def _tma_describable(dt, size, perm):
+    """From the plan summary: fused rank <= 5, a true transpose, and every
+    stride of A and B other than the unit one a multiple of 16 bytes."""
+    import re
+    d = h.inspect_plan(dt, size, perm)
+    sa = [int(x) for x in re.search(r"strides A: (.*)", d).group(1).split()]
+    sb = [int(x) for x in re.search(r"strides B: (.*)", d).group(1).split()]
+    pm = [int(x) for x in re.search(r"perm \(output dim -> input dim\): (.*)", d).group(1).split()]
+    esz = {"f32": 4, "f64": 8, "c64": 8}[dt]
+    return (len(sa) <= 5 and pm[0] != 0 and all(v * esz % 16 == 0 for v in sa[1:]) and
+            all(v * esz % 16 == 0 for k, v in enumerate(sb) if k != pm[0]))
+
+
+@pytest.mark.parametrize("seed", range(24))
+def test_replay_ttile_random(seed):
+    dt, size, perm = _random_ttile_case(seed)
+    assert _tma_describable(dt, size, perm), (dt, size, perm)
+    rc, n = check(dt, size, perm)
+    assert rc == 0, (dt, size, perm, rc)
+    assert n == np.prod(size)
