@@ -179,3 +179,41 @@ def test_tma_tile_plain_workload(tmp_path):
                 assert_same(got, want, name, f"boxes={kx}x{ky} stages={stages}")
     finally:
         h.tune_cache_clear()
+
+
+def _random_case(seed):
+    """A seeded problem a TMA tile can serve (the CPU replay's generator):
+    input dim 0 and the output's leading dim in multiples of 16 bytes."""
+    rng = np.random.default_rng(seed)
+    name = ["f32", "f64", "c64"][seed % 3]
+    q = 4 if name == "f32" else 2
+    rank = int(rng.integers(2, 6))
+    while True:
+        perm = [int(x) for x in rng.permutation(rank)]
+        if perm[0] != 0:
+            break
+    size = [int(rng.integers(2, 9)) for _ in range(rank)]
+    size[0] = q * int(rng.integers(1, 12))
+    size[perm[0]] = q * int(rng.integers(1, 12))
+    return name, size, perm
+
+
+@pytest.mark.parametrize("seed", range(12))
+def test_tma_tile_random_shapes(tmp_path, seed):
+    name, size, perm = _random_case(seed)
+    rng = np.random.default_rng(900 + seed)
+    n = int(np.prod(size))
+    a = seeded(rng, n, name)
+    b0 = seeded(rng, n, name)
+    try:
+        for al, be in ((1.0, 0.0), (2.3, 4.2)):
+            want = oracle_run(name, size, perm, al, be, a, b0)
+            path, key, f = _cache_line(tmp_path, name, size, perm, None, None, al, be, None)
+            for kx, ky, order, stages in ((1, 1, 0, 1), (2, 1, 1, 3)):
+                _force(path, key, f, kx, ky, order, stages)
+                got, desc = _run(name, size, perm, None, None, al, be, a, b0, 0)
+                assert "TMA tile" in desc, desc
+                assert_same(got, want, name, f"seed {seed} {size} {perm} a={al} b={be} "
+                                             f"boxes={kx}x{ky} stages={stages}")
+    finally:
+        h.tune_cache_clear()
