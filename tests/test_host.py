@@ -100,3 +100,18 @@ def test_bench_roofline_picks_the_dominant_kernel(monkeypatch, tmp_path):
     # the committed traffic file parses into per-kernel ratios
     t = bench._profiled_traffic()
     assert t is None or all(0.5 < v < 2.0 for v in t.values())
+
+
+def test_bench_roofline_names_the_tma_kernels(monkeypatch):
+    """A plan on either TMA-tile form is timed and named as its own kernel
+    (no DRAM-traffic ratio is committed for them: traffic stays null)."""
+    import bench
+    assert {"tile", "vtile", "ttile", "ttile_pipe", "rows"} <= set(bench.KERNEL_OF_KIND)
+    plans = [(None, 10**9, "ttile", {}), (None, 10**9, "ttile_pipe", {}),
+             (None, 10**9, "tile", {})]
+    kind_ms = {"ttile": 4.0, "ttile_pipe": 6.0, "tile": 3.0}
+    monkeypatch.setattr(bench, "_peaks", lambda: (6000.0, "measured"))
+    r = bench._roofline(plans, kind_ms, 2, {"k_tile": 1.0})
+    assert r["kernel"] == "k_ttile_pipe"
+    assert r["traffic"] is None
+    assert set(r["kernels"]) == {"k_ttile", "k_ttile_pipe", "k_tile"}
