@@ -74,7 +74,8 @@ struct TileParams {
 
 // Whether a TMA tile (KIND_TTILE) can serve this problem: fused rank 2-5,
 // 4- or 8-byte elements, no shared stride-1 dim, every stride other than the
-// unit one a multiple of 16 bytes and below 2^40 bytes, extents below 2^32.
+// unit one a multiple of 16 bytes and below 2^40 bytes, extents below 2^31
+// (box coordinates are signed 32-bit).
 bool ttile_possible(const HpttProblem &p);
 
 // The tensor map of one side of a KIND_TTILE tile: side 0 is A with its dims
