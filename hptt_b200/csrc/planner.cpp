@@ -783,8 +783,10 @@ bool ttile_possible(const HpttProblem &p) {
   const int sz = elem_bytes(p.dtype);
   if ((sz != 4 && sz != 8) || p.rank < 2 || p.rank > 5 || p.perm[0] == 0) return false;
   for (int d = 0; d < p.rank; ++d) {
-    // TMA box coordinates are signed 32-bit
-    if (p.n[d] < 1 || p.n[d] > 0x7fffffffLL) return false;
+    // TMA box coordinates are signed 32-bit: a tile's origin plus its box
+    // offsets (under 2^10) must stay positive, so extents stay at or below
+    // 2^30
+    if (p.n[d] < 1 || p.n[d] > (int64_t(1) << 30)) return false;
     if (d > 0 && ((p.sA[d] * sz) % 16 != 0 || p.sA[d] * sz >= (int64_t(1) << 40))) return false;
     if (d != p.perm[0] && ((p.sB[d] * sz) % 16 != 0 || p.sB[d] * sz >= (int64_t(1) << 40)))
       return false;

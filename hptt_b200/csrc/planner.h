@@ -74,7 +74,7 @@ struct TileParams {
 
 // Whether a TMA tile (KIND_TTILE) can serve this problem: fused rank 2-5,
 // 4- or 8-byte elements, no shared stride-1 dim, every stride other than the
-// unit one a multiple of 16 bytes and below 2^40 bytes, extents below 2^31
+// unit one a multiple of 16 bytes and below 2^40 bytes, extents at most 2^30
 // (box coordinates are signed 32-bit).
 bool ttile_possible(const HpttProblem &p);
 
